@@ -1,0 +1,161 @@
+/*
+ * mmffb200 -- C ABI of the B200-native batched MMFF94/94s conformer optimizer.
+ *
+ * Plain C types only: every pointer below is a CUDA device pointer owned by
+ * the caller (a PyTorch tensor, a cudaMalloc arena, ...), every call is
+ * ordered on the given stream and returns 0 on success or a negative
+ * MMFFB_E* code; mmffb_last_error() gives the message of the calling thread's
+ * last failure.
+ *
+ * Data layout (written by mlxmolkit_b200/pack.py):
+ *   mol_desc   int32[n_mols * MMFFB_MOL_DESC_INTS], fields MMFFB_MD_*
+ *   bonded     16-byte records in chunks of 32 terms per term type; within
+ *              a chunk no two terms share an atom in the same role
+ *   atom_cls   int32 per atom: non-bonded class (index into the molecule's
+ *              ncls x ncls (R*, eps) table at cls_tab + 2*cls_off)
+ *   atom_q     float64 per atom: MMFF partial charge (|q| <= 1e-10 stored as 0)
+ *   pair_mask  uint32 bit rows: N rows x ceil(N/32) words of "non-bonded
+ *              pair (i<j)" bits, then the same for "1-4 pair" bits
+ *   positions  float32, conformer c's 3N coordinates at pos + conf_coord[c]
+ */
+#ifndef MMFFB200_H
+#define MMFFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *mmffb_stream_t; /* = cudaStream_t */
+
+enum {
+    MMFFB_OK = 0,
+    MMFFB_EINVAL = -1,   /* bad argument (size, pointer, unsupported option) */
+    MMFFB_ECUDA = -2,    /* CUDA runtime error (message in mmffb_last_error) */
+    MMFFB_ESCRATCH = -3, /* scratch buffer smaller than mmffb_*_scratch_bytes */
+    MMFFB_ETOOBIG = -4   /* molecule larger than the kernel supports */
+};
+
+/* molecule descriptor fields */
+enum {
+    MMFFB_MD_N = 0, MMFFB_MD_ATOM_OFF, MMFFB_MD_NCLS, MMFFB_MD_CLS_OFF, MMFFB_MD_MASK_OFF,
+    MMFFB_MD_DIEL, MMFFB_MD_B_OFF, MMFFB_MD_B_NCH, MMFFB_MD_A_OFF, MMFFB_MD_A_NCH,
+    MMFFB_MD_S_OFF, MMFFB_MD_S_NCH, MMFFB_MD_O_OFF, MMFFB_MD_O_NCH, MMFFB_MD_T_OFF,
+    MMFFB_MD_T_NCH, MMFFB_MOL_DESC_INTS
+};
+
+/* per-conformer exit status; 0, 2, 3 and 5 are the reference's status 0 ("done") */
+enum {
+    MMFFB_ST_GRAD = 0,       /* gradient test passed */
+    MMFFB_ST_MAXIT = 1,      /* iteration cap reached (the reference's status 1) */
+    MMFFB_ST_TOLX = 2,       /* step below TOLX */
+    MMFFB_ST_SLOPE = 3,      /* no descent direction (slope >= 0) */
+    MMFFB_ST_NONFINITE = 4,  /* energy or gradient not finite */
+    MMFFB_ST_LSFAIL = 5      /* line search found no decrease; position restored */
+};
+
+/* arithmetic of the optimizer */
+enum {
+    MMFFB_PREC_MIXED = 0, /* FP32 terms, gradients, BFGS update; FP64 energy sums, Armijo, tests */
+    MMFFB_PREC_FP64 = 1,  /* everything FP64 (the GPU oracle) */
+    MMFFB_PREC_FP32 = 2   /* everything FP32 */
+};
+
+typedef struct {
+    int32_t n_mols;
+    int32_t max_atoms;           /* largest N in the batch */
+    const int32_t *mol_desc;
+    const void *bonded;          /* 16-byte aligned records */
+    const int32_t *atom_cls;
+    const double *atom_q;
+    const float *cls_tab;        /* (R*, eps) float pairs */
+    const uint32_t *pair_mask;
+} MMFFBatchDev;
+
+typedef struct {
+    int32_t n_conf;
+    int32_t max_atoms;           /* largest N among these conformers */
+    const int32_t *conf_mol;     /* molecule of each conformer */
+    const int64_t *conf_coord;   /* float offset of each conformer's coordinates */
+    const int32_t *order;        /* processing order (largest first) or NULL */
+} MMFFConfDev;
+
+typedef struct {
+    int32_t max_iters;
+    int32_t history_m;           /* 0: dense BFGS; > 0: L-BFGS with that many pairs */
+    int32_t precision;           /* MMFFB_PREC_* */
+    int32_t threads;             /* CTA size 64, 128 or 256; 0 = choose from max_atoms */
+    int32_t ctas_per_sm;         /* persistent CTAs per SM; 0 = as many as fit */
+    float grad_tol;
+    double consts[8];            /* TOLX FUNCTOL MOVETOL EPS MAXSTEP_FACTOR MAX_LS GRAD_SCALE GRAD_CAP */
+    double mode[4];              /* cb (per degree), angle/oop prefactor, stretch-bend gradient prefactor, honour linear */
+    int32_t exit_test;           /* MMFFB_EXIT_* */
+    int32_t check_every;         /* MMFFB_EXIT_ATOM_NORM: test every k-th iteration (0 = every) */
+    float atom_grad_scale;       /* MMFFB_EXIT_ATOM_NORM: factor on the raw gradient */
+} MMFFOptParams;
+
+/* convergence test of mmffb_minimize */
+enum {
+    MMFFB_EXIT_TG = 0,        /* max|g_i|*max(|x_i|,1)/max(E*gradScale,1) < grad_tol (tg.metal:300-316) */
+    MMFFB_EXIT_ATOM_NORM = 1  /* max over atoms |g_atom|*atom_grad_scale <= grad_tol, every check_every
+                                 iterations (mmff_metal_optimizer.py:334-359, 405-416) */
+};
+
+int mmffb_version(void);
+const char *mmffb_last_error(void);
+
+/*
+ * Energy and (if grad != NULL) gradient of every conformer at pos.
+ * Replaces the mega kernel mmff_energy_grad_metal_mega
+ * (mlxmolkit/mmff_metal_kernel.py:713-744) and the serial/parallel energy
+ * macros of the in-kernel optimizer (mlxmolkit/mmff_bfgs_source_tg.metal:54-113).
+ * energy: float64[n_conf]; grad: float32 laid out like pos.
+ */
+int mmffb_energy_grad(const MMFFBatchDev *batch, const MMFFConfDev *confs, int32_t precision,
+                      const double *mode, const float *pos, double *energy, float *grad,
+                      mmffb_stream_t stream);
+
+/* Bytes of device scratch mmffb_minimize needs for these conformers and options. */
+size_t mmffb_minimize_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs,
+                                    const MMFFOptParams *opt);
+
+/*
+ * Minimise every conformer in place (one persistent, work-queued launch):
+ * dense BFGS (history_m == 0) or L-BFGS, backtracking line search, TOLX and
+ * gradient exits inside the kernel.  Replaces the in-kernel optimizers behind
+ * mmff_minimize_nk (mlxmolkit/mmff_minimize.py:231-346;
+ * mmff_bfgs_source_tg.metal, mmff_lbfgs_source_tg.metal).
+ * energy: float64[n_conf]; status, iters: int32[n_conf]; ls_evals (may be
+ * NULL): int32[n_conf] energy-only line-search evaluations per conformer.
+ */
+int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                   float *pos, double *energy, int32_t *status, int32_t *iters, int32_t *ls_evals,
+                   void *scratch, size_t scratch_bytes, mmffb_stream_t stream);
+
+/*
+ * The reference's own design restated in CUDA, kept as the measured
+ * "plain one-launch-per-batch FP32 GPU path": 32 threads per conformer,
+ * serial thread-0 gradient, 32-wide energy, inverse Hessian in global memory,
+ * one launch for the batch (mlxmolkit/mmff_bfgs_source_tg.metal:1-372).
+ */
+size_t mmffb_plain_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs);
+int mmffb_plain_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                         float *pos, double *energy, int32_t *status, int32_t *iters,
+                         void *scratch, size_t scratch_bytes, mmffb_stream_t stream);
+
+/*
+ * Barzilai-Borwein steepest descent with the energy guard and per-atom step
+ * cap of the reference's fused optimizer (mlxmolkit/mmff_metal_kernel.py:792-1150),
+ * behind mmff_optimize_metal_fused_multi_mol.  opt->max_iters iterations;
+ * sd[0] = max_step (A), sd[1] = grad_lr.
+ */
+int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                   const float *sd, float *pos, double *energy, mmffb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MMFFB200_H */

@@ -1,0 +1,200 @@
+// C ABI entry points and launch planning (host code).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "mmff_kernels.cuh"
+
+namespace mmffb {
+
+static thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    return fail(MMFFB_ECUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+static int device_props(int *sms, int *smem_optin) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    e = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+    e = cudaDeviceGetAttribute(smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(smem)");
+    return 0;
+}
+
+static int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c) {
+    if (!b || !c) return fail(MMFFB_EINVAL, "null batch or conformer descriptor");
+    if (c->n_conf < 0 || b->n_mols < 0) return fail(MMFFB_EINVAL, "negative count");
+    if (c->n_conf > 0 && (!b->mol_desc || !b->bonded || !b->atom_cls || !b->atom_q || !b->cls_tab ||
+                          !b->pair_mask || !c->conf_mol || !c->conf_coord))
+        return fail(MMFFB_EINVAL, "null device pointer in batch");
+    if (c->max_atoms <= 0 && c->n_conf > 0) return fail(MMFFB_EINVAL, "max_atoms must be positive");
+    if (c->max_atoms > kMaxAtoms) return fail(MMFFB_ETOOBIG, "molecule of %d atoms exceeds %d", c->max_atoms, kMaxAtoms);
+    return 0;
+}
+
+static TermMode to_mode(const double *mode) {
+    TermMode md;
+    md.cb = mode[0]; md.kang = mode[1]; md.ksbg = mode[2]; md.lin = mode[3] != 0.0;
+    return md;
+}
+
+static KConst to_consts(const double *k) {
+    KConst K;
+    K.tolx = k[0]; K.functol = k[1]; K.movetol = k[2]; K.eps = k[3]; K.maxstep = k[4];
+    K.maxls = (int)k[5]; K.gscale = k[6]; K.gcap = k[7];
+    return K;
+}
+
+// Pick the kernel instance (CTA size, register-cached H columns, matrix in
+// shared or global memory) and the persistent grid for these conformers.
+static int plan_minimize(const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl) {
+    int sms = 0, optin = 0;
+    int r = device_props(&sms, &optin);
+    if (r) return r;
+    const int nmax = c->max_atoms;
+    const int n = 3 * nmax;
+    const bool mixed = o->precision == MMFFB_PREC_MIXED;
+    if (o->precision < 0 || o->precision > 2) return fail(MMFFB_EINVAL, "unknown precision %d", o->precision);
+    const size_t rs = o->precision == MMFFB_PREC_FP64 ? 8 : 4;
+    const size_t as = o->precision == MMFFB_PREC_FP32 ? 4 : 8;
+    if (o->history_m < 0 || o->history_m > kMaxHist) return fail(MMFFB_EINVAL, "history_m out of range");
+    const bool lb = o->history_m > 0;
+    int nt = o->threads;
+    if (nt == 0) nt = nmax <= 24 ? 64 : (nmax <= 48 ? 128 : 256);
+    if (nt != 64 && nt != 128 && nt != 256) return fail(MMFFB_EINVAL, "threads must be 64, 128 or 256");
+    if (!mixed || lb) nt = 256;
+    if (!lb && n > 512) return fail(MMFFB_ETOOBIG, "dense BFGS supports up to 170 atoms (got %d); use L-BFGS", nmax);
+    Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as);
+    bool msm = Ls.total <= (size_t)optin;
+    int nc = 2;
+    if (!lb) {
+        if (msm) {
+            if (nt == 64 && n > 128) nt = 128;
+            nc = nt == 64 ? 4 : 8;
+            if (n > 32 * nc) msm = false;
+        }
+        if (!msm) { nt = 256; nc = 16; }
+    }
+    Layout L = make_layout(nmax, nt / 32, o->history_m, msm, rs, as);
+    if (L.total > (size_t)optin)
+        return fail(MMFFB_ETOOBIG, "molecule of %d atoms needs %zu B of shared memory", nmax, L.total);
+    pl->nt = nt;
+    pl->nc = nc;
+    pl->msm = msm;
+    pl->smem = L.total;
+    pl->rsz = rs;
+    pl->gslot = mat_elems(nmax, o->history_m);
+    int fit = o->precision == MMFFB_PREC_FP64 ? occupancy_fp64(*pl, lb)
+            : o->precision == MMFFB_PREC_FP32 ? occupancy_fp32(*pl, lb) : occupancy_mixed(*pl, lb);
+    if (fit < 0) return fit;
+    if (fit < 1) return fail(MMFFB_ETOOBIG, "no CTA of this instance fits on an SM (%zu B shared)", pl->smem);
+    if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
+    int grid = sms * fit;
+    if (grid > c->n_conf) grid = c->n_conf > 0 ? c->n_conf : 1;
+    pl->grid = grid;
+    return 0;
+}
+
+}  // namespace mmffb
+
+using namespace mmffb;
+
+extern "C" {
+
+int mmffb_version(void) { return 1; }
+
+const char *mmffb_last_error(void) { return g_err.c_str(); }
+
+int mmffb_energy_grad(const MMFFBatchDev *batch, const MMFFConfDev *confs, int32_t precision,
+                      const double *mode, const float *pos, double *energy, float *grad,
+                      mmffb_stream_t stream) {
+    int r = check_batch(batch, confs);
+    if (r) return r;
+    if (!mode || !pos || !energy) return fail(MMFFB_EINVAL, "null mode, pos or energy");
+    if (confs->n_conf == 0) return 0;
+    Params P;
+    memset(&P, 0, sizeof P);
+    P.b = *batch;
+    P.c = *confs;
+    P.md = to_mode(mode);
+    P.nmax = confs->max_atoms;
+    P.pos = const_cast<float *>(pos);
+    P.energy = energy;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (precision == MMFFB_PREC_FP64) return energy_grad_fp64(P, grad, st);
+    if (precision == MMFFB_PREC_FP32) return energy_grad_fp32(P, grad, st);
+    if (precision != MMFFB_PREC_MIXED) return fail(MMFFB_EINVAL, "unknown precision %d", precision);
+    return energy_grad_mixed(P, grad, st);
+}
+
+size_t mmffb_minimize_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs,
+                                    const MMFFOptParams *opt) {
+    if (check_batch(batch, confs) || !opt) return 0;
+    Plan pl;
+    if (plan_minimize(confs, opt, &pl)) return 0;
+    size_t b = 256;
+    if (!pl.msm) b += (size_t)pl.grid * pl.gslot * pl.rsz;
+    return b;
+}
+
+int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                   float *pos, double *energy, int32_t *status, int32_t *iters, int32_t *ls_evals,
+                   void *scratch, size_t scratch_bytes, mmffb_stream_t stream) {
+    int r = check_batch(batch, confs);
+    if (r) return r;
+    if (!opt || !pos || !energy || !status || !iters) return fail(MMFFB_EINVAL, "null argument");
+    if (opt->max_iters < 0) return fail(MMFFB_EINVAL, "max_iters must be >= 0");
+    if (opt->consts[5] < 1) return fail(MMFFB_EINVAL, "MAX_LS must be >= 1");
+    if (opt->exit_test != MMFFB_EXIT_TG && opt->exit_test != MMFFB_EXIT_ATOM_NORM)
+        return fail(MMFFB_EINVAL, "unknown exit_test %d", opt->exit_test);
+    if (confs->n_conf == 0) return 0;
+    Plan pl;
+    r = plan_minimize(confs, opt, &pl);
+    if (r) return r;
+    size_t need = 256 + (pl.msm ? 0 : (size_t)pl.grid * pl.gslot * pl.rsz);
+    if (!scratch || scratch_bytes < need)
+        return fail(MMFFB_ESCRATCH, "scratch of %zu B given, %zu B needed", scratch_bytes, need);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 256, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    Params P;
+    memset(&P, 0, sizeof P);
+    P.b = *batch;
+    P.c = *confs;
+    P.md = to_mode(opt->mode);
+    P.K = to_consts(opt->consts);
+    P.max_iters = opt->max_iters;
+    P.hist_m = opt->history_m;
+    P.grad_tol = opt->grad_tol;
+    P.exit_test = opt->exit_test;
+    P.check_every = opt->check_every;
+    P.atom_grad_scale = opt->atom_grad_scale;
+    P.ls_evals = ls_evals;
+    P.nmax = confs->max_atoms;
+    P.pos = pos;
+    P.energy = energy;
+    P.status = status;
+    P.iters = iters;
+    P.counter = reinterpret_cast<int *>(scratch);
+    P.gmat = reinterpret_cast<unsigned char *>(scratch) + 256;
+    P.gslot = pl.gslot;
+    if (opt->precision == MMFFB_PREC_FP64) return minimize_fp64(P, pl, st);
+    if (opt->precision == MMFFB_PREC_FP32) return minimize_fp32(P, pl, st);
+    return minimize_mixed(P, pl, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,851 @@
+#pragma once
+// B200 (sm_100a) kernels of the batched MMFF94/94s conformer optimizer.
+//
+// Work unit: one conformer, owned by one CTA for its whole optimisation.
+// A persistent grid pulls conformers from a global work counter (largest
+// first), so a conformer that converges early frees its CTA for the next
+// one instead of idling until the slowest member of a lockstep batch ends.
+//
+// Per conformer, shared memory holds the coordinates (float4 per atom), the
+// optimizer vectors, per-warp gradient buffers, per-atom non-bonded class and
+// charge, and -- when it fits -- the dense inverse Hessian (or the L-BFGS
+// history); otherwise the matrix lives in a per-CTA global slot that stays
+// resident in the 126 MB L2.
+//
+// Energy / gradient:
+//  * bonded terms arrive in chunks of 32 records; inside a chunk no two terms
+//    share an atom in the same role, so each role's gradient scatter is a
+//    plain conflict-free read-modify-write into the warp's private buffer;
+//  * non-bonded pairs are not read from a pair table: warp w walks rows i of
+//    the upper triangle, lanes take j, a bit row marks the non-bonded pairs
+//    (topological distance >= 3) and the 1-4 pairs, (R*, eps) comes from the
+//    molecule's class x class table and q_i q_j from per-atom charges;
+//  * the gradient is the fixed-order sum of the per-warp buffers and the
+//    energy a fixed-order FP64 (mixed precision) reduction, so results are
+//    bit-reproducible run to run.
+//
+// Dense BFGS: the rank-2 inverse-Hessian update of iteration k is applied
+// lazily inside iteration k+1's single pass over H, which also forms both
+// matrix-vector products (H g and H dg): one read and one write of H per
+// iteration.  The direction -H_{k+1} g follows from H_k g and vector terms.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "mmff_terms.cuh"
+#include "mmffb200.h"
+
+namespace mmffb {
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *where);
+
+constexpr int kMaxHist = 16;       // L-BFGS history pairs supported
+constexpr int kMaxAtoms = 1024;    // atom indices are packed as 16 bits; smem bounds this further
+
+struct MolV {
+    int n, atom_off, ncls, cls_off, mask_off, diel;
+    int boff, bnch, aoff, anch, soff, snch, ooff, onch, toff, tnch;
+};
+
+__device__ __forceinline__ MolV load_mol(const int32_t *desc, int m) {
+    const int32_t *d = desc + (size_t)m * MMFFB_MOL_DESC_INTS;
+    MolV v;
+    v.n = d[MMFFB_MD_N]; v.atom_off = d[MMFFB_MD_ATOM_OFF]; v.ncls = d[MMFFB_MD_NCLS];
+    v.cls_off = d[MMFFB_MD_CLS_OFF]; v.mask_off = d[MMFFB_MD_MASK_OFF]; v.diel = d[MMFFB_MD_DIEL];
+    v.boff = d[MMFFB_MD_B_OFF]; v.bnch = d[MMFFB_MD_B_NCH]; v.aoff = d[MMFFB_MD_A_OFF];
+    v.anch = d[MMFFB_MD_A_NCH]; v.soff = d[MMFFB_MD_S_OFF]; v.snch = d[MMFFB_MD_S_NCH];
+    v.ooff = d[MMFFB_MD_O_OFF]; v.onch = d[MMFFB_MD_O_NCH]; v.toff = d[MMFFB_MD_T_OFF];
+    v.tnch = d[MMFFB_MD_T_NCH];
+    return v;
+}
+
+struct KConst {
+    double tolx, functol, movetol, eps, maxstep, gscale, gcap;
+    int maxls;
+};
+
+struct Params {
+    MMFFBatchDev b;
+    MMFFConfDev c;
+    TermMode md;
+    KConst K;
+    int max_iters;
+    int hist_m;
+    float grad_tol;
+    int exit_test;
+    int check_every;
+    float atom_grad_scale;
+    int32_t *ls_evals;
+    int nmax;          // largest atom count of the launch (shared-memory layout)
+    float *pos;
+    double *energy;
+    int32_t *status;
+    int32_t *iters;
+    void *gmat;        // per-CTA global matrix slots (when not in shared memory)
+    size_t gslot;      // elements per slot
+    int *counter;      // work counter
+};
+
+__host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared-memory layout of one CTA (byte offsets).
+struct Layout {
+    size_t pos4, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, red, rho, alpha, mat, total;
+};
+
+__host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, bool mat_in_smem,
+                                              size_t rs, size_t as) {
+    Layout L;
+    size_t nv = (size_t)((3 * nmax + 3) & ~3);
+    size_t o = 0;
+    L.pos4 = o; o = al16(o + 4 * (size_t)nmax * rs);
+    L.x = o; o = al16(o + nv * rs);
+    L.g = o; o = al16(o + nv * rs);
+    L.dir = o; o = al16(o + nv * rs);
+    L.xo = o; o = al16(o + nv * rs);
+    L.dg = o; o = al16(o + nv * rs);
+    L.hp = o; o = al16(o + nv * rs);
+    L.hq = o; o = al16(o + nv * rs);
+    L.pxi = o; o = al16(o + nv * rs);
+    L.pc = o; o = al16(o + nv * rs);
+    L.pr = o; o = al16(o + nv * rs);
+    L.gbuf = o; o = al16(o + (size_t)nwarps * nv * rs);
+    L.cls = o; o = al16(o + (size_t)nmax * 4);
+    L.q = o; o = al16(o + (size_t)nmax * 8);
+    L.red = o; o = al16(o + 2 * (size_t)nwarps * 8 * as);
+    L.rho = o; o = al16(o + kMaxHist * as);
+    L.alpha = o; o = al16(o + kMaxHist * as);
+    L.mat = o;
+    if (mat_in_smem) {
+        size_t me = hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)(3 * nmax);
+        o = al16(o + me * rs);
+    }
+    L.total = o;
+    return L;
+}
+
+__host__ __device__ inline size_t mat_elems(int nmax, int hist_m) {
+    size_t nv = (size_t)((3 * nmax + 3) & ~3);
+    return hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)(3 * nmax);
+}
+
+template <class R> __device__ __forceinline__ R qprod(double a, double b);
+template <> __device__ __forceinline__ float qprod<float>(double a, double b) { return (float)(a * b); }
+// the term lists carry q_i*q_j rounded to float32 (mmff_params.py:305,318); every precision uses it
+template <> __device__ __forceinline__ double qprod<double>(double a, double b) { return (double)(float)(a * b); }
+
+template <class T> __device__ __forceinline__ T wsum(T v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <class T> __device__ __forceinline__ T wmax(T v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) { T u = __shfl_xor_sync(0xffffffffu, v, o); v = u > v ? u : v; }
+    return v;
+}
+
+// Block reduction of KS sums and KM maxima; every thread receives the results.
+// One __syncthreads: the caller alternates between two scratch halves.
+template <int NW, int KS, int KM, class A>
+__device__ __forceinline__ void block_reduce(A (&s)[KS], A (&m)[KM], A *red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < KS; ++k) s[k] = wsum(s[k]);
+#pragma unroll
+    for (int k = 0; k < KM; ++k) m[k] = wmax(m[k]);
+    constexpr int K = KS + KM;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < KS; ++k) red[warp * K + k] = s[k];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) red[warp * K + KS + k] = m[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+        A t = A(0);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) t += red[w * K + k];
+        s[k] = t;
+    }
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        A t = red[KS + k];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) { A u = red[w * K + KS + k]; t = u > t ? u : t; }
+        m[k] = t;
+    }
+}
+
+template <class R> __device__ __forceinline__ void add3(R *dst, const R *f) {
+    dst[0] += f[0]; dst[1] += f[1]; dst[2] += f[2];
+}
+
+__device__ __forceinline__ float u2f(uint32_t u) { return __uint_as_float(u); }
+
+// Energy (thread partial, not reduced) and -- if G -- per-warp gradient buffers.
+// pos4: smem float4-strided coordinates; gbuf: NW x nv; cls/qa: per atom.
+template <class R, class A, int NW, bool G>
+__device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R *pos4, R *gbuf,
+                                        const int *cls, const double *qa, int nv) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int N = m.n;
+    A acc = A(0);
+    R *gw = gbuf + (size_t)warp * nv;
+    if (G) {
+        for (int k = lane; k < 3 * N; k += 32) gw[k] = R(0);
+        __syncwarp();
+    }
+    const uint4 *BR = reinterpret_cast<const uint4 *>(P.b.bonded);
+    const TermMode md = P.md;
+
+    for (int c = warp; c < m.bnch; c += NW) {
+        uint4 r = __ldg(BR + m.boff + (size_t)c * 32 + lane);
+        bool v = r.x != 0xffffffffu;
+        int i = r.x & 0xffff, j = r.x >> 16;
+        R f[2][3];
+        if (v) acc += (A)bond_term<R, G>(pos4 + 4 * i, pos4 + 4 * j, (R)u2f(r.y), (R)u2f(r.z), f);
+        if (G) {
+            if (v) add3(gw + 3 * i, f[0]);
+            __syncwarp();
+            if (v) add3(gw + 3 * j, f[1]);
+            __syncwarp();
+        }
+    }
+    for (int c = warp; c < m.anch; c += NW) {
+        uint4 r = __ldg(BR + m.aoff + (size_t)c * 32 + lane);
+        bool v = r.x != 0xffffffffu;
+        int i = r.x & 0xffff, j = r.x >> 16, k = r.y & 0xffff;
+        bool lin = (r.y >> 16) != 0;
+        R f[3][3];
+        if (v)
+            acc += (A)angle_term<R, G>(pos4 + 4 * i, pos4 + 4 * j, pos4 + 4 * k, (R)u2f(r.z), (R)u2f(r.w),
+                                       lin, md, f);
+        if (G) {
+            if (v) add3(gw + 3 * i, f[0]);
+            __syncwarp();
+            if (v) add3(gw + 3 * j, f[1]);
+            __syncwarp();
+            if (v) add3(gw + 3 * k, f[2]);
+            __syncwarp();
+        }
+    }
+    for (int c = warp; c < m.snch; c += NW) {
+        uint4 r0 = __ldg(BR + m.soff + (size_t)c * 64 + lane);
+        uint4 r1 = __ldg(BR + m.soff + (size_t)c * 64 + 32 + lane);
+        bool v = r0.x != 0xffffffffu;
+        int i = r0.x & 0xffff, j = r0.x >> 16, k = (int)r0.y;
+        R f[3][3];
+        if (v)
+            acc += (A)strbend_term<R, G>(pos4 + 4 * i, pos4 + 4 * j, pos4 + 4 * k, (R)u2f(r0.z), (R)u2f(r0.w),
+                                         (R)u2f(r1.x), (R)u2f(r1.y), (R)u2f(r1.z), md, f);
+        if (G) {
+            if (v) add3(gw + 3 * i, f[0]);
+            __syncwarp();
+            if (v) add3(gw + 3 * j, f[1]);
+            __syncwarp();
+            if (v) add3(gw + 3 * k, f[2]);
+            __syncwarp();
+        }
+    }
+    for (int c = warp; c < m.onch; c += NW) {
+        uint4 r = __ldg(BR + m.ooff + (size_t)c * 32 + lane);
+        bool v = r.x != 0xffffffffu;
+        int i = r.x & 0xffff, j = r.x >> 16, k = r.y & 0xffff, l = r.y >> 16;
+        R f[4][3];
+        if (v)
+            acc += (A)oop_term<R, G>(pos4 + 4 * i, pos4 + 4 * j, pos4 + 4 * k, pos4 + 4 * l, (R)u2f(r.z), md, f);
+        if (G) {
+            if (v) add3(gw + 3 * i, f[0]);
+            __syncwarp();
+            if (v) add3(gw + 3 * j, f[1]);
+            __syncwarp();
+            if (v) add3(gw + 3 * k, f[2]);
+            __syncwarp();
+            if (v) add3(gw + 3 * l, f[3]);
+            __syncwarp();
+        }
+    }
+    for (int c = warp; c < m.tnch; c += NW) {
+        uint4 r0 = __ldg(BR + m.toff + (size_t)c * 64 + lane);
+        uint4 r1 = __ldg(BR + m.toff + (size_t)c * 64 + 32 + lane);
+        bool v = r0.x != 0xffffffffu;
+        int i = r0.x & 0xffff, j = r0.x >> 16, k = r0.y & 0xffff, l = r0.y >> 16;
+        R f[4][3];
+        if (v)
+            acc += (A)torsion_term<R, G>(pos4 + 4 * i, pos4 + 4 * j, pos4 + 4 * k, pos4 + 4 * l, (R)u2f(r0.z),
+                                         (R)u2f(r0.w), (R)u2f(r1.x), f);
+        if (G) {
+            if (v) add3(gw + 3 * i, f[0]);
+            __syncwarp();
+            if (v) add3(gw + 3 * j, f[1]);
+            __syncwarp();
+            if (v) add3(gw + 3 * k, f[2]);
+            __syncwarp();
+            if (v) add3(gw + 3 * l, f[3]);
+            __syncwarp();
+        }
+    }
+
+    // non-bonded pairs, implicit from the bit rows
+    const int W = (N + 31) >> 5;
+    const uint32_t *pm = P.b.pair_mask + m.mask_off;
+    const uint32_t *p14 = pm + (size_t)N * W;
+    const float2 *tab = reinterpret_cast<const float2 *>(P.b.cls_tab) + m.cls_off;
+    const bool dd = m.diel == 2;
+    for (int i = warp; i < N - 1; i += NW) {
+        const R xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
+        const int ci = cls[i] * m.ncls;
+        const double qi = qa[i];
+        R fx = R(0), fy = R(0), fz = R(0);
+        for (int jb = (i + 1) & ~31; jb < N; jb += 32) {
+            const uint32_t wd = __ldg(pm + (size_t)i * W + (jb >> 5));
+            if (wd == 0u) continue;
+            if ((wd >> lane) & 1u) {
+                const int j = jb + lane;
+                const uint32_t w14 = __ldg(p14 + (size_t)i * W + (jb >> 5));
+                const float2 t = __ldg(tab + ci + cls[j]);
+                R qq = qprod<R>(qi, qa[j]);
+                if ((w14 >> lane) & 1u) qq *= R(0.75);
+                const R dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+                R ev, ee, s;
+                pair_term<R, G>(dx, dy, dz, (R)t.x, (R)t.y, qq, dd, ev, ee, s);
+                acc += (A)ev;
+                acc += (A)ee;
+                if (G) {
+                    const R gx = s * dx, gy = s * dy, gz = s * dz;
+                    fx += gx; fy += gy; fz += gz;
+                    gw[3 * j] -= gx; gw[3 * j + 1] -= gy; gw[3 * j + 2] -= gz;
+                }
+            }
+        }
+        if (G) {
+            __syncwarp();
+            fx = wsum(fx); fy = wsum(fy); fz = wsum(fz);
+            if (lane == 0) { gw[3 * i] += fx; gw[3 * i + 1] += fy; gw[3 * i + 2] += fz; }
+            __syncwarp();
+        }
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// The persistent optimizer kernel
+// ---------------------------------------------------------------------------
+
+template <class R, class A, int NT, int NC, bool MSM, bool LB>
+struct Opt {
+    static constexpr int NW = NT / 32;
+    const Params &P;
+    R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *gbuf, *mat;
+    int *cls;
+    double *qa;
+    A *red, *rho_s, *alpha_s;
+    int rsel;
+    MolV m;
+    int N, n, nv;
+
+    __device__ Opt(const Params &p, unsigned char *sm) : P(p), rsel(0) {
+        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A));
+        pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
+        xo = (R *)(sm + L.xo); dg = (R *)(sm + L.dg); hp = (R *)(sm + L.hp); hq = (R *)(sm + L.hq);
+        pxi = (R *)(sm + L.pxi); pc = (R *)(sm + L.pc); pr = (R *)(sm + L.pr); gbuf = (R *)(sm + L.gbuf);
+        cls = (int *)(sm + L.cls); qa = (double *)(sm + L.q); red = (A *)(sm + L.red);
+        rho_s = (A *)(sm + L.rho); alpha_s = (A *)(sm + L.alpha);
+        if (MSM) mat = (R *)(sm + L.mat);
+        else mat = (R *)p.gmat + (size_t)blockIdx.x * p.gslot;
+    }
+
+    __device__ __forceinline__ A *next_red() {
+        A *r = red + rsel * NW * 8;
+        rsel ^= 1;
+        return r;
+    }
+
+    template <int KS, int KM>
+    __device__ __forceinline__ void reduce(A (&s)[KS], A (&mm)[KM]) {
+        block_reduce<NW, KS, KM, A>(s, mm, next_red());
+    }
+
+    __device__ __forceinline__ A energy() {
+        A e[1] = {eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv)};
+        A z[1] = {A(0)};
+        reduce<1, 1>(e, z);
+        return e[0];
+    }
+
+    // gradient at pos4 into dst (raw, unscaled); needs a preceding __syncthreads after pos4 writes
+    __device__ __forceinline__ void gradient(R *dst) {
+        eval_terms<R, A, NW, true>(P, m, pos4, gbuf, cls, qa, nv);
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += NT) {
+            R s = R(0);
+#pragma unroll
+            for (int w = 0; w < NW; ++w) s += gbuf[(size_t)w * nv + k];
+            dst[k] = s;
+        }
+    }
+
+    __device__ __forceinline__ void setpos(int k, R v) { pos4[4 * (k / 3) + (k % 3)] = v; }
+
+    // One pass over the dense inverse Hessian: apply the pending rank-2 update
+    // H_ij += pxi_j*pr_i + pxi_i*pc_j, store, and form hp = H g, hq = H dg.
+    __device__ __forceinline__ void hpass(bool pending) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        R cx[NC], cc[NC], cg[NC], cd[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int j = lane + 32 * c;
+            const bool in = j < n;
+            cx[c] = in ? pxi[j] : R(0);
+            cc[c] = in ? pc[j] : R(0);
+            cg[c] = in ? g[j] : R(0);
+            cd[c] = in ? dg[j] : R(0);
+        }
+        for (int i = warp; i < n; i += NW) {
+            R *row = mat + (size_t)i * n;
+            const R ri = pending ? pr[i] : R(0), xi = pending ? pxi[i] : R(0);
+            R ap = R(0), aq = R(0);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int j = lane + 32 * c;
+                if (j < n) {
+                    R h = row[j];
+                    if (pending) {
+                        h = fma(cx[c], ri, h);
+                        h = fma(xi, cc[c], h);
+                        row[j] = h;
+                    }
+                    ap = fma(h, cg[c], ap);
+                    aq = fma(h, cd[c], aq);
+                }
+            }
+            ap = wsum(ap);
+            aq = wsum(aq);
+            if (lane == 0) { hp[i] = ap; hq[i] = aq; }
+        }
+    }
+
+    // L-BFGS two-loop recursion (lbfgs_tg.metal:264-292): dir = -H g from the ring history
+    __device__ __forceinline__ void two_loop(int hcount, int hidx) {
+        const int hm = P.hist_m;
+        R *S = mat, *Y = mat + (size_t)hm * nv;
+        for (int k = threadIdx.x; k < n; k += NT) hq[k] = g[k];
+        for (int jj = hcount - 1; jj >= 0; --jj) {
+            int slot = ((hidx - 1 - (hcount - 1 - jj)) % hm + hm) % hm;
+            const R *Sj = S + (size_t)slot * nv;
+            A s1[1] = {A(0)}, z[1] = {A(0)};
+            for (int k = threadIdx.x; k < n; k += NT) s1[0] += (A)(Sj[k] * hq[k]);
+            reduce<1, 1>(s1, z);
+            A aj = rho_s[slot] * s1[0];
+            if (threadIdx.x == 0) alpha_s[jj] = aj;
+            const R *Yj = Y + (size_t)slot * nv;
+            const R ar = (R)aj;
+            for (int k = threadIdx.x; k < n; k += NT) hq[k] -= ar * Yj[k];
+        }
+        if (hcount > 0) {
+            int nw = ((hidx - 1) % hm + hm) % hm;
+            const R *Sn = S + (size_t)nw * nv, *Yn = Y + (size_t)nw * nv;
+            A s2[2] = {A(0), A(0)}, z[1] = {A(0)};
+            for (int k = threadIdx.x; k < n; k += NT) {
+                s2[0] += (A)(Sn[k] * Yn[k]);
+                s2[1] += (A)(Yn[k] * Yn[k]);
+            }
+            reduce<2, 1>(s2, z);
+            const R gam = (R)(s2[0] / (s2[1] > A(1e-30) ? s2[1] : A(1e-30)));
+            for (int k = threadIdx.x; k < n; k += NT) hq[k] *= gam;
+        }
+        for (int jj = 0; jj < hcount; ++jj) {
+            int slot = ((hidx - 1 - (hcount - 1 - jj)) % hm + hm) % hm;
+            const R *Yj = Y + (size_t)slot * nv, *Sj = S + (size_t)slot * nv;
+            A s1[1] = {A(0)}, z[1] = {A(0)};
+            for (int k = threadIdx.x; k < n; k += NT) s1[0] += (A)(Yj[k] * hq[k]);
+            reduce<1, 1>(s1, z);
+            const A bj = rho_s[slot] * s1[0];
+            const R c = (R)(alpha_s[jj] - bj);
+            for (int k = threadIdx.x; k < n; k += NT) hq[k] += c * Sj[k];
+        }
+        for (int k = threadIdx.x; k < n; k += NT) dir[k] = -hq[k];
+    }
+
+    __device__ void run(int conf) {
+        const int tid = threadIdx.x;
+        const KConst &K = P.K;
+        m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
+        N = m.n;
+        n = 3 * N;
+        nv = (3 * P.nmax + 3) & ~3;
+        const float *gp = P.pos + P.c.conf_coord[conf];
+        for (int k = tid; k < n; k += NT) {
+            R v = (R)gp[k];
+            x[k] = v;
+            setpos(k, v);
+        }
+        for (int a = tid; a < N; a += NT) {
+            cls[a] = P.b.atom_cls[m.atom_off + a];
+            qa[a] = P.b.atom_q[m.atom_off + a];
+        }
+        if (!LB) {
+            for (size_t e = tid; e < (size_t)n * n; e += NT) {
+                const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
+                mat[e] = i == j ? R(1) : R(0);
+            }
+        }
+        __syncthreads();
+
+        // initial gradient and scale (header :435-454, tg.metal:115-122)
+        gradient(hp);
+        A gs_[2] = {A(0), A(0)}, gm_[1] = {A(0)};
+        for (int k = tid; k < n; k += NT) {
+            gs_[0] += (A)fabs(hp[k]);
+            gs_[1] += (A)(x[k] * x[k]);
+            A a = (A)fabs(hp[k]);
+            gm_[0] = a > gm_[0] ? a : gm_[0];
+        }
+        reduce<2, 1>(gs_, gm_);
+        R gsc = (R)K.gscale;
+        {
+            // bounded: a non-finite gradient is caught below, never halved forever
+            R mx = (R)gm_[0] * gsc;
+            for (int h = 0; h < 256 && mx > (R)K.gcap; ++h) { mx *= R(0.5); gsc *= R(0.5); }
+        }
+        for (int k = tid; k < n; k += NT) {
+            R v = hp[k] * gsc;
+            g[k] = v;
+            dir[k] = -v;
+        }
+        A E = energy();
+        const A max_step = (A)K.maxstep * (sqrt(gs_[1]) > (A)n ? sqrt(gs_[1]) : (A)n);
+        int status = MMFFB_ST_MAXIT;
+        int it = 0, done_iters = 0, nevals = 0;
+        bool pending = false;
+        int hcount = 0, hidx = 0;
+        if (!isfinite((double)E) || !isfinite((double)gs_[0])) {
+            status = MMFFB_ST_NONFINITE;
+            it = P.max_iters;
+        } else {
+            for (it = 0; it < P.max_iters; ++it) {
+                // direction length, slope, largest relative component; xold = x
+                A s3[2] = {A(0), A(0)}, m3[1] = {A(0)};
+                for (int k = tid; k < n; k += NT) {
+                    const R d = dir[k], xv = x[k];
+                    xo[k] = xv;
+                    s3[0] += (A)(d * d);
+                    s3[1] += (A)(d * g[k]);
+                    A t = (A)(fabs(d) / fmax(fabs(xv), R(1)));
+                    m3[0] = t > m3[0] ? t : m3[0];
+                }
+                reduce<2, 1>(s3, m3);
+                const A dn = sqrt(s3[0]);
+                if (dn > max_step) {
+                    const R sc = (R)(max_step / dn);
+                    A s4[1] = {A(0)}, m4[1] = {A(0)};
+                    for (int k = tid; k < n; k += NT) {
+                        const R d = dir[k] * sc;
+                        dir[k] = d;
+                        s4[0] += (A)(d * g[k]);
+                        A t = (A)(fabs(d) / fmax(fabs(x[k]), R(1)));
+                        m4[0] = t > m4[0] ? t : m4[0];
+                    }
+                    reduce<1, 1>(s4, m4);
+                    s3[1] = s4[0];
+                    m3[0] = m4[0];
+                }
+                const A slope = s3[1];
+                if (!(slope < A(0))) { status = MMFFB_ST_SLOPE; break; }
+                const A lam_min = (A)K.movetol / (m3[0] > A(1e-30) ? m3[0] : A(1e-30));
+
+                // backtracking line search (tg.metal:192-256)
+                const A Eold = E;
+                A lam = A(1), plam = A(1), pe = Eold;
+                bool ok = false;
+                for (int ls = 0; ls < K.maxls; ++ls) {
+                    if (lam < lam_min) break;
+                    ++nevals;
+                    const R lr = (R)lam;
+                    for (int k = tid; k < n; k += NT) {
+                        const R v = xo[k] + lr * dir[k];
+                        x[k] = v;
+                        setpos(k, v);
+                    }
+                    __syncthreads();
+                    const A et = energy();
+                    if (et - Eold <= (A)K.functol * lam * slope) { E = et; ok = true; break; }
+                    A tl;
+                    if (ls == 0) {
+                        tl = -slope / (A(2) * (et - Eold - slope));
+                    } else {
+                        const A r1 = et - Eold - lam * slope, r2 = pe - Eold - plam * slope;
+                        const A l2 = lam * lam, p2 = plam * plam, dv = lam - plam;
+                        if (fabs(dv) < A(1e-30)) tl = A(0.5) * lam;
+                        else {
+                            const A a = (r1 / l2 - r2 / p2) / dv, b = (-plam * r1 / l2 + lam * r2 / p2) / dv;
+                            if (fabs(a) < A(1e-30)) tl = fabs(b) > A(1e-30) ? -slope / (A(2) * b) : A(0.5) * lam;
+                            else {
+                                const A disc = b * b - A(3) * a * slope;
+                                if (disc < A(0)) tl = A(0.5) * lam;
+                                else if (b <= A(0)) tl = (-b + sqrt(disc)) / (A(3) * a);
+                                else tl = -slope / (b + sqrt(disc));
+                            }
+                        }
+                    }
+                    tl = tl < A(0.5) * lam ? tl : A(0.5) * lam;
+                    tl = tl > A(0.1) * lam ? tl : A(0.1) * lam;
+                    plam = lam; pe = et; lam = tl;
+                }
+                if (!ok) {
+                    for (int k = tid; k < n; k += NT) {
+                        x[k] = xo[k];
+                        setpos(k, xo[k]);
+                    }
+                    __syncthreads();
+                }
+                // xi = x - xold, TOLX (kept per thread until the next reduction)
+                A tolx = A(0);
+                for (int k = tid; k < n; k += NT) {
+                    const R xi = x[k] - xo[k];
+                    xo[k] = xi;
+                    A t = (A)(fabs(xi) / fmax(fabs(x[k]), R(1)));
+                    tolx = t > tolx ? t : tolx;
+                }
+                // gradient at the new point (computed before the TOLX verdict; one
+                // wasted evaluation per conformer instead of a barrier per iteration)
+                gradient(hp);
+                const bool atom_test = P.exit_test == MMFFB_EXIT_ATOM_NORM &&
+                                       (P.check_every <= 1 || (it + 1) % P.check_every == 0);
+                A anorm = A(0);
+                if (atom_test) {
+                    __syncthreads();
+                    for (int a = tid; a < N; a += NT) {
+                        const R gx = hp[3 * a], gy = hp[3 * a + 1], gz = hp[3 * a + 2];
+                        const A v = (A)sqrt(gx * gx + gy * gy + gz * gz);
+                        anorm = v > anorm ? v : anorm;
+                    }
+                }
+                A gs2[1] = {A(0)}, gm2[4] = {A(0), A(0), tolx, anorm};
+                for (int k = tid; k < n; k += NT) {
+                    const A a = (A)fabs(hp[k]);
+                    gs2[0] += a;
+                    gm2[0] = a > gm2[0] ? a : gm2[0];
+                    const A b = (A)(fabs(hp[k]) * fmax(fabs(x[k]), R(1)));
+                    gm2[1] = b > gm2[1] ? b : gm2[1];
+                }
+                reduce<1, 4>(gs2, gm2);
+                if (!isfinite((double)gs2[0]) || !isfinite((double)E)) { status = MMFFB_ST_NONFINITE; break; }
+                if (atom_test && gm2[3] * (A)P.atom_grad_scale <= (A)P.grad_tol) { status = MMFFB_ST_GRAD; break; }
+                if (gm2[2] < (A)K.tolx) { status = ok ? MMFFB_ST_TOLX : MMFFB_ST_LSFAIL; break; }
+                {
+                    R mx = (R)gm2[0] * gsc;
+                    for (int h = 0; h < 256 && mx > (R)K.gcap; ++h) { mx *= R(0.5); gsc *= R(0.5); }
+                }
+                if (P.exit_test == MMFFB_EXIT_TG) {
+                    const A num = (A)((R)gm2[1] * gsc);
+                    A den = E * (A)gsc;
+                    den = den > A(1) ? den : A(1);
+                    if (num / den < (A)P.grad_tol) { status = MMFFB_ST_GRAD; break; }
+                }
+                for (int k = tid; k < n; k += NT) {
+                    const R gn = hp[k] * gsc;
+                    dg[k] = gn - g[k];
+                    g[k] = gn;
+                }
+                if (!LB) {
+                    __syncthreads();
+                    hpass(pending);
+                    __syncthreads();
+                    A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};
+                    for (int k = tid; k < n; k += NT) {
+                        const R dgk = dg[k], xik = xo[k], qk = hq[k], gk = g[k];
+                        d6[0] += (A)(dgk * xik);
+                        d6[1] += (A)(dgk * qk);
+                        d6[2] += (A)(dgk * dgk);
+                        d6[3] += (A)(xik * xik);
+                        d6[4] += (A)(xik * gk);
+                        d6[5] += (A)(qk * gk);
+                    }
+                    reduce<6, 1>(d6, z);
+                    const A fac = d6[0], fae = d6[1];
+                    if (fac * fac > (A)K.eps * d6[2] * d6[3] && fac > A(0)) {
+                        const A fi = A(1) / fac;
+                        const A al = fi * (A(1) + fae * fi);
+                        const R cxg = (R)(al * d6[4]), cqg = (R)(fi * d6[5]), fxg = (R)(fi * d6[4]);
+                        const R rfi = (R)fi, ral = (R)al;
+                        for (int k = tid; k < n; k += NT) {
+                            const R xk = xo[k], qk = hq[k];
+                            dir[k] = -(hp[k] + cxg * xk - cqg * xk - fxg * qk);
+                            pxi[k] = xk;
+                            pc[k] = -rfi * qk;
+                            pr[k] = ral * xk - rfi * qk;
+                        }
+                        pending = true;
+                    } else {
+                        for (int k = tid; k < n; k += NT) dir[k] = -hp[k];
+                        pending = false;
+                    }
+                } else {
+                    // L-BFGS history update (lbfgs_tg.metal:247-262)
+                    A y1[1] = {A(0)}, z[1] = {A(0)};
+                    for (int k = tid; k < n; k += NT) y1[0] += (A)(dg[k] * xo[k]);
+                    reduce<1, 1>(y1, z);
+                    if (y1[0] > A(1e-10)) {
+                        const int hm = P.hist_m;
+                        const int slot = hidx % hm;
+                        R *S = mat + (size_t)slot * nv, *Y = mat + (size_t)hm * nv + (size_t)slot * nv;
+                        for (int k = tid; k < n; k += NT) { S[k] = xo[k]; Y[k] = dg[k]; }
+                        if (tid == 0) rho_s[slot] = A(1) / y1[0];
+                        hidx++;
+                        if (hcount < hm) hcount++;
+                    }
+                    __syncthreads();
+                    two_loop(hcount, hidx);
+                }
+            }
+        }
+        if (status != MMFFB_ST_NONFINITE || it < P.max_iters)
+            done_iters = it < P.max_iters ? it + (status == MMFFB_ST_SLOPE ? 0 : 1) : P.max_iters;
+        __syncthreads();
+        float *op = P.pos + P.c.conf_coord[conf];
+        for (int k = tid; k < n; k += NT) op[k] = (float)x[k];
+        if (tid == 0) {
+            P.energy[conf] = (double)E;
+            P.status[conf] = status;
+            P.iters[conf] = done_iters;
+            if (P.ls_evals) P.ls_evals[conf] = nevals;
+        }
+        __syncthreads();
+    }
+};
+
+template <class R, class A, int NT, int NC, bool MSM, bool LB>
+__global__ void __launch_bounds__(NT) minimize_kernel(const Params P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_item;
+    Opt<R, A, NT, NC, MSM, LB> opt(P, smem);
+    const int *order = P.c.order;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= P.c.n_conf) break;
+        opt.run(order ? order[item] : item);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Energy + gradient of every conformer (one CTA each)
+// ---------------------------------------------------------------------------
+
+template <class R, class A, int NT>
+__global__ void __launch_bounds__(NT) energy_grad_kernel(const Params P, float *grad) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NW = NT / 32;
+    const int conf = blockIdx.x;
+    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A));
+    R *pos4 = (R *)(smem + L.pos4), *gbuf = (R *)(smem + L.gbuf);
+    int *cls = (int *)(smem + L.cls);
+    double *qa = (double *)(smem + L.q);
+    A *red = (A *)(smem + L.red);
+    const MolV m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
+    const int n = 3 * m.n, nv = (3 * P.nmax + 3) & ~3;
+    const float *gp = P.pos + P.c.conf_coord[conf];
+    for (int k = threadIdx.x; k < n; k += NT) pos4[4 * (k / 3) + (k % 3)] = (R)gp[k];
+    for (int a = threadIdx.x; a < m.n; a += NT) {
+        cls[a] = P.b.atom_cls[m.atom_off + a];
+        qa[a] = P.b.atom_q[m.atom_off + a];
+    }
+    __syncthreads();
+    A e[1], z[1] = {A(0)};
+    if (grad) e[0] = eval_terms<R, A, NW, true>(P, m, pos4, gbuf, cls, qa, nv);
+    else e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv);
+    block_reduce<NW, 1, 1, A>(e, z, red);
+    if (grad) {
+        float *go = grad + P.c.conf_coord[conf];
+        for (int k = threadIdx.x; k < n; k += NT) {
+            R s = R(0);
+#pragma unroll
+            for (int w = 0; w < NW; ++w) s += gbuf[(size_t)w * nv + k];
+            go[k] = (float)s;
+        }
+    }
+    if (threadIdx.x == 0) P.energy[conf] = (double)e[0];
+}
+
+// launch plan of a minimisation
+struct Plan {
+    int nt, nc;
+    bool msm;
+    size_t smem;
+    int grid;
+    size_t gslot;      // matrix elements per CTA slot when not in shared memory
+    size_t rsz;
+};
+
+template <class R, class A, int NT, int NC, bool MSM, bool LB>
+int launch_min(const Params &P, const Plan &pl, cudaStream_t st) {
+    auto k = minimize_kernel<R, A, NT, NC, MSM, LB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    k<<<pl.grid, NT, pl.smem, st>>>(P);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "minimize_kernel launch");
+    return 0;
+}
+
+template <class R, class A, int NT>
+int launch_eg(const Params &P, float *grad, cudaStream_t st) {
+    Layout L = make_layout(P.nmax, NT / 32, 0, false, sizeof(R), sizeof(A));
+    auto k = energy_grad_kernel<R, A, NT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    k<<<P.c.n_conf, NT, L.total, st>>>(P, grad);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "energy_grad_kernel launch");
+    return 0;
+}
+
+template <class R, class A, int NT, int NC, bool MSM, bool LB>
+int occ_min(const Plan &pl) {
+    auto k = minimize_kernel<R, A, NT, NC, MSM, LB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, pl.smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    return n;
+}
+
+struct LaunchFn {
+    const Params &P;
+    const Plan &pl;
+    cudaStream_t st;
+    template <class R, class A, int NT, int NC, bool MSM, bool LB> int run() const {
+        return launch_min<R, A, NT, NC, MSM, LB>(P, pl, st);
+    }
+};
+
+struct OccFn {
+    const Plan &pl;
+    template <class R, class A, int NT, int NC, bool MSM, bool LB> int run() const {
+        return occ_min<R, A, NT, NC, MSM, LB>(pl);
+    }
+};
+
+// per-precision instantiation units (mmff_inst_*.cu)
+int minimize_mixed(const Params &P, const Plan &pl, cudaStream_t st);
+int minimize_fp64(const Params &P, const Plan &pl, cudaStream_t st);
+int minimize_fp32(const Params &P, const Plan &pl, cudaStream_t st);
+int occupancy_mixed(const Plan &pl, bool lb);
+int occupancy_fp64(const Plan &pl, bool lb);
+int occupancy_fp32(const Plan &pl, bool lb);
+int energy_grad_mixed(const Params &P, float *grad, cudaStream_t st);
+int energy_grad_fp64(const Params &P, float *grad, cudaStream_t st);
+int energy_grad_fp32(const Params &P, float *grad, cudaStream_t st);
+
+}  // namespace mmffb

@@ -1,0 +1,85 @@
+"""ctypes binding of libmmffb200.so (the C ABI declared in include/mmffb200.h).
+
+The shared library is the only compute path: importing this module on a
+machine without the built library, or calling it without a CUDA device,
+raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmmffb200.so")
+
+P = ctypes.c_void_p
+
+MMFFB_OK, MMFFB_EINVAL, MMFFB_ECUDA, MMFFB_ESCRATCH, MMFFB_ETOOBIG = 0, -1, -2, -3, -4
+ST_GRAD, ST_MAXIT, ST_TOLX, ST_SLOPE, ST_NONFINITE, ST_LSFAIL = 0, 1, 2, 3, 4, 5
+STATUS_NAMES = {0: "grad", 1: "max_iters", 2: "tolx", 3: "slope", 4: "nonfinite", 5: "line_search"}
+PREC = {"mixed": 0, "fp64": 1, "fp32": 2}
+EXIT_TG, EXIT_ATOM_NORM = 0, 1
+
+
+class MMFFBatchDev(ctypes.Structure):
+    _fields_ = [("n_mols", ctypes.c_int32), ("max_atoms", ctypes.c_int32),
+                ("mol_desc", P), ("bonded", P), ("atom_cls", P), ("atom_q", P),
+                ("cls_tab", P), ("pair_mask", P)]
+
+
+class MMFFConfDev(ctypes.Structure):
+    _fields_ = [("n_conf", ctypes.c_int32), ("max_atoms", ctypes.c_int32),
+                ("conf_mol", P), ("conf_coord", P), ("order", P)]
+
+
+class MMFFOptParams(ctypes.Structure):
+    _fields_ = [("max_iters", ctypes.c_int32), ("history_m", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("grad_tol", ctypes.c_float),
+                ("consts", ctypes.c_double * 8), ("mode", ctypes.c_double * 4),
+                ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
+                ("atom_grad_scale", ctypes.c_float)]
+
+
+EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
+           "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd"]
+
+_lib = None
+
+
+class MMFFBError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the library (raises when it is missing: there is no other compute path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MMFFBError(f"{LIB_PATH} is missing: build it with `make -C csrc` "
+                         "(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    BP, CP, OP = ctypes.POINTER(MMFFBatchDev), ctypes.POINTER(MMFFConfDev), ctypes.POINTER(MMFFOptParams)
+    L.mmffb_version.restype = ctypes.c_int
+    L.mmffb_last_error.restype = ctypes.c_char_p
+    L.mmffb_energy_grad.restype = ctypes.c_int
+    L.mmffb_energy_grad.argtypes = [BP, CP, ctypes.c_int32, P, P, P, P, P]
+    L.mmffb_minimize_scratch_bytes.restype = ctypes.c_size_t
+    L.mmffb_minimize_scratch_bytes.argtypes = [BP, CP, OP]
+    L.mmffb_minimize.restype = ctypes.c_int
+    L.mmffb_minimize.argtypes = [BP, CP, OP, P, P, P, P, P, P, ctypes.c_size_t, P]
+    L.mmffb_plain_scratch_bytes.restype = ctypes.c_size_t
+    L.mmffb_plain_scratch_bytes.argtypes = [BP, CP]
+    L.mmffb_plain_minimize.restype = ctypes.c_int
+    L.mmffb_plain_minimize.argtypes = [BP, CP, OP, P, P, P, P, P, ctypes.c_size_t, P]
+    L.mmffb_fused_sd.restype = ctypes.c_int
+    L.mmffb_fused_sd.argtypes = [BP, CP, OP, P, P, P, P]
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str) -> None:
+    if rc != MMFFB_OK:
+        msg = load().mmffb_last_error().decode(errors="replace")
+        raise MMFFBError(f"{what} failed ({rc}): {msg}")

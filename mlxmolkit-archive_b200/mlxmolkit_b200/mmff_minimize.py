@@ -1,0 +1,368 @@
+"""Batched MMFF94/94s minimisation on B200 -- the ``mmff_minimize_nk`` drop-in.
+
+Host side of the C ABI in include/mmffb200.h: term tables are packed once per
+molecule (``pack.py``), uploaded with PyTorch (device memory, streams), and
+the sm_100a kernels of libmmffb200.so do the work.  Nothing here computes
+energies on the CPU; without the library or a CUDA device the calls raise.
+
+Reference counterparts:
+  mmff_minimize_nk          mlxmolkit/mmff_minimize.py:231-346
+  optimizer constants       mlxmolkit/mmff_bfgs_header.metal:3-12
+  status -> converged       mlxmolkit/mmff_minimize.py:346 (status == 0)
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .pack import PackedBatch, conformer_index, lpt_order, pack_molecules
+
+# Optimizer constants TOLX FUNCTOL MOVETOL EPS MAX_STEP_FACTOR MAX_LS GRAD_SCALE GRAD_CAP:
+# the reference in-kernel optimizer's (mmff_bfgs_header.metal:3-12) and RDKit's / nvMolKit's
+# (mlxmolkit/bfgs_metal.py:23-28).
+TG_CONSTS = (1.2e-6, 1e-4, 1e-6, 3e-7, 100.0, 1000.0, 0.1, 10.0)
+RDKIT_CONSTS = (1.2e-7, 1e-4, 1e-7, 3e-8, 100.0, 100.0, 0.1, 10.0)
+# Term constants {cb, angle/oop prefactor, stretch-bend gradient prefactor, honour linear}:
+# in-kernel optimizer header (mmff_bfgs_header.metal:85-87,154,192) and mega/fused kernels
+# (mmff_metal_kernel.py:274-280).
+MODE_TG = (-0.4 * math.pi / 180.0, 143.9325 * (math.pi / 180.0) ** 2, 143.9325 * math.pi / 180.0, 1.0)
+MODE_MEGA = (-0.007, 0.043844, 2.51210, 0.0)
+LBFGS_M = 8                    # mlxmolkit/mmff_minimize.py:31
+LBFGS_ATOM_THRESHOLD = 150     # mlxmolkit/conformer_pipeline_v2.py:448
+
+CONVERGED_STATUSES = (_lib.ST_GRAD, _lib.ST_TOLX, _lib.ST_SLOPE, _lib.ST_LSFAIL)
+
+
+def load_tuning(path: Optional[str] = None) -> dict:
+    """Per-bin launch configuration written by autotune.py (empty if none)."""
+    import json
+    import os
+    path = path or os.environ.get("MMFFB_TUNING") or os.path.join(os.path.dirname(__file__), "tuning.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("bins", {})
+    except (OSError, ValueError):
+        return {}
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.MMFFBError("no CUDA device: the MMFF kernels run on the GPU only")
+    return torch
+
+
+class DeviceBatch:
+    """Packed molecule tables resident in device memory (one upload, many launches)."""
+
+    def __init__(self, packed: PackedBatch, device=None):
+        torch = _torch()
+        self.packed = packed
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev, non_blocking=False)
+        self.mol_desc = t(packed.mol_desc.reshape(-1))
+        self.bonded = t(packed.bonded.view(np.int32).reshape(-1))
+        self.atom_cls = t(packed.atom_cls if len(packed.atom_cls) else np.zeros(1, np.int32))
+        self.atom_q = t(packed.atom_q if len(packed.atom_q) else np.zeros(1, np.float64))
+        self.cls_tab = t(packed.cls_tab.reshape(-1))
+        self.pair_mask = t(packed.pair_mask.view(np.int32))
+        self.n_atoms = packed.n_atoms
+
+    @classmethod
+    def from_params(cls, params_list, device=None) -> "DeviceBatch":
+        return cls(pack_molecules(params_list), device)
+
+    def desc(self) -> _lib.MMFFBatchDev:
+        return _lib.MMFFBatchDev(self.packed.n_mols, self.packed.max_atoms, self.mol_desc.data_ptr(),
+                                 self.bonded.data_ptr(), self.atom_cls.data_ptr(), self.atom_q.data_ptr(),
+                                 self.cls_tab.data_ptr(), self.pair_mask.data_ptr())
+
+
+class DeviceConformers:
+    """Conformer -> molecule map, coordinate offsets and processing order on the device."""
+
+    def __init__(self, batch: DeviceBatch, conf_mol: np.ndarray, conf_coord: np.ndarray,
+                 order: Optional[np.ndarray] = None):
+        torch = _torch()
+        dev = batch.device
+        self.n_conf = int(len(conf_mol))
+        self.conf_mol_np = np.asarray(conf_mol, dtype=np.int32)
+        self.max_atoms = int(batch.n_atoms[self.conf_mol_np].max()) if self.n_conf else 1
+        self.conf_mol = torch.from_numpy(self.conf_mol_np.copy()).to(dev)
+        self.conf_coord = torch.from_numpy(np.asarray(conf_coord, dtype=np.int64).copy()).to(dev)
+        self.order = None if order is None else torch.from_numpy(np.asarray(order, np.int32).copy()).to(dev)
+
+    def desc(self) -> _lib.MMFFConfDev:
+        return _lib.MMFFConfDev(self.n_conf, self.max_atoms, self.conf_mol.data_ptr(),
+                                self.conf_coord.data_ptr(), 0 if self.order is None else self.order.data_ptr())
+
+
+def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: str = "mixed",
+               consts=TG_CONSTS, mode=MODE_TG, threads: int = 0, ctas_per_sm: int = 0,
+               exit_test: int = _lib.EXIT_TG, check_every: int = 0,
+               atom_grad_scale: float = 1.0) -> _lib.MMFFOptParams:
+    o = _lib.MMFFOptParams()
+    o.exit_test = int(exit_test)
+    o.check_every = int(check_every)
+    o.atom_grad_scale = float(atom_grad_scale)
+    o.max_iters = int(max_iters)
+    o.history_m = int(history_m)
+    o.precision = _lib.PREC[precision]
+    o.threads = int(threads)
+    o.ctas_per_sm = int(ctas_per_sm)
+    o.grad_tol = float(grad_tol)
+    for i, v in enumerate(consts):
+        o.consts[i] = float(v)
+    for i, v in enumerate(mode):
+        o.mode[i] = float(v)
+    return o
+
+
+def _stream_ptr(torch, stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+@dataclass
+class MinimizeResult:
+    positions: np.ndarray      # float32, flat, molecule-major conformer order
+    energies: np.ndarray       # float64 (C,)
+    status: np.ndarray         # int32 (C,) MMFFB_ST_*
+    iters: np.ndarray          # int32 (C,)
+
+    @property
+    def converged(self) -> np.ndarray:
+        return np.isin(self.status, CONVERGED_STATUSES)
+
+
+class Minimizer:
+    """Device-resident minimisation of one packed batch (tables uploaded once)."""
+
+    def __init__(self, params_list, conf_counts: Sequence[int], device=None):
+        self.params_list = list(params_list)
+        self.conf_counts = [int(k) for k in conf_counts]
+        self.batch = DeviceBatch.from_params(self.params_list, device)
+        n_atoms = [int(p.n_atoms) for p in self.params_list]
+        self.conf_mol, self.conf_coord, self.total = conformer_index(n_atoms, self.conf_counts)
+        self.order = lpt_order(n_atoms, self.conf_mol)
+        self.confs = DeviceConformers(self.batch, self.conf_mol, self.conf_coord, self.order)
+        self._scratch = None
+
+    def _scratch_for(self, nbytes: int):
+        torch = _torch()
+        if self._scratch is None or self._scratch.numel() < nbytes:
+            self._scratch = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.batch.device)
+        return self._scratch
+
+    def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
+                        precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
+                        ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
+                        atom_grad_scale: float = 1.0, stream=None, out=None, evals=None):
+        """Minimise in place on the device; returns (energy, status, iters) device tensors.
+
+        ``evals`` (optional int32 device tensor, one per conformer) receives the
+        number of energy-only line-search evaluations.
+        """
+        torch = _torch()
+        L = _lib.load()
+        C = self.confs.n_conf
+        if out is None:
+            e = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+            st = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+            it = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+        else:
+            e, st, it = out
+        o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode, threads, ctas_per_sm,
+                       exit_test, check_every, atom_grad_scale)
+        bd, cd = self.batch.desc(), self.confs.desc()
+        nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
+        if nbytes == 0 and C > 0:
+            _lib.check(-1 if not L.mmffb_last_error() else _lib.MMFFB_EINVAL, "mmffb_minimize_scratch_bytes")
+        scratch = self._scratch_for(nbytes)
+        rc = L.mmffb_minimize(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), pos_dev.data_ptr(),
+                              e.data_ptr(), st.data_ptr(), it.data_ptr(),
+                              evals.data_ptr() if evals is not None else None, scratch.data_ptr(),
+                              scratch.numel(), _stream_ptr(torch, stream))
+        _lib.check(rc, "mmffb_minimize")
+        return e, st, it
+
+    def minimize(self, positions: np.ndarray, **kw) -> MinimizeResult:
+        torch = _torch()
+        pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+        if pos.size != self.total:
+            raise ValueError(f"positions hold {pos.size} floats, the conformers need {self.total}")
+        pos_dev = torch.from_numpy(pos.copy()).to(self.batch.device)
+        e, st, it = self.minimize_device(pos_dev, **kw)
+        torch.cuda.synchronize()
+        return MinimizeResult(pos_dev.cpu().numpy(), e.cpu().numpy(), st.cpu().numpy(), it.cpu().numpy())
+
+    def plain_minimize(self, positions: np.ndarray, *, max_iters: int, grad_tol: float = 1e-4,
+                       consts=TG_CONSTS, mode=MODE_TG) -> MinimizeResult:
+        """The reference design restated (32 threads per conformer, serial gradient, global H)."""
+        torch = _torch()
+        L = _lib.load()
+        pos_dev = torch.from_numpy(np.ascontiguousarray(positions, np.float32).reshape(-1).copy()).to(
+            self.batch.device)
+        out = self.plain_device(pos_dev, max_iters=max_iters, grad_tol=grad_tol, consts=consts, mode=mode)
+        torch.cuda.synchronize()
+        e, st, it = out
+        return MinimizeResult(pos_dev.cpu().numpy(), e.cpu().numpy(), st.cpu().numpy(), it.cpu().numpy())
+
+    def plain_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, consts=TG_CONSTS,
+                     mode=MODE_TG, stream=None):
+        torch = _torch()
+        L = _lib.load()
+        C = self.confs.n_conf
+        plain_confs = DeviceConformers(self.batch, self.conf_mol, self.conf_coord, None)
+        bd, cd = self.batch.desc(), plain_confs.desc()
+        o = opt_params(max_iters, grad_tol, 0, "fp32", consts, mode)
+        nbytes = L.mmffb_plain_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd))
+        scratch = self._scratch_for(nbytes)
+        e = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        st = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+        it = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+        rc = L.mmffb_plain_minimize(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), pos_dev.data_ptr(),
+                                    e.data_ptr(), st.data_ptr(), it.data_ptr(), scratch.data_ptr(),
+                                    scratch.numel(), _stream_ptr(torch, stream))
+        _lib.check(rc, "mmffb_plain_minimize")
+        return e, st, it
+
+    def energy_grad(self, positions: np.ndarray, precision: str = "mixed", mode=MODE_TG, want_grad=True):
+        """Energy (float64) and gradient (float32, flat) of every conformer."""
+        torch = _torch()
+        L = _lib.load()
+        pos_dev = torch.from_numpy(np.ascontiguousarray(positions, np.float32).reshape(-1).copy()).to(
+            self.batch.device)
+        C = self.confs.n_conf
+        e = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        g = torch.zeros_like(pos_dev) if want_grad else None
+        md = (ctypes.c_double * 4)(*[float(v) for v in mode])
+        bd, cd = self.batch.desc(), self.confs.desc()
+        rc = L.mmffb_energy_grad(ctypes.byref(bd), ctypes.byref(cd), _lib.PREC[precision], md,
+                                 pos_dev.data_ptr(), e.data_ptr(), g.data_ptr() if g is not None else None,
+                                 _stream_ptr(torch))
+        _lib.check(rc, "mmffb_energy_grad")
+        torch.cuda.synchronize()
+        return e.cpu().numpy(), (g.cpu().numpy() if g is not None else None)
+
+    def fused_sd(self, positions: np.ndarray, *, max_iters: int, max_step: float, grad_lr: float,
+                 mode=MODE_MEGA):
+        """Barzilai-Borwein steepest descent of the reference's fused optimizer."""
+        torch = _torch()
+        L = _lib.load()
+        pos_dev = torch.from_numpy(np.ascontiguousarray(positions, np.float32).reshape(-1).copy()).to(
+            self.batch.device)
+        C = self.confs.n_conf
+        e = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        o = opt_params(max_iters, 0.0, 0, "mixed", TG_CONSTS, mode)
+        sd = (ctypes.c_float * 2)(float(max_step), float(grad_lr))
+        bd, cd = self.batch.desc(), self.confs.desc()
+        rc = L.mmffb_fused_sd(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), sd, pos_dev.data_ptr(),
+                              e.data_ptr(), _stream_ptr(torch))
+        _lib.check(rc, "mmffb_fused_sd")
+        torch.cuda.synchronize()
+        return pos_dev.cpu().numpy(), e.cpu().numpy()
+
+
+DEFAULT_BINS = (24, 42, 74, 170, 1024)   # atom-count upper bounds of the size classes
+
+
+class BinnedMinimizer(Minimizer):
+    """Size-binned launch: conformers grouped by atom count, one launch per bin.
+
+    Each bin gets the kernel instance that suits its molecules (small bins:
+    fewer threads per conformer, inverse Hessian in shared memory, several
+    CTAs per SM; large bins: 256 threads, Hessian in an L2-resident global
+    slot) and its own CUDA stream, so the bins run concurrently and fill the
+    SMs each other leaves idle.  ``tuning`` maps a bin's upper bound to
+    {"threads": ..., "ctas_per_sm": ...} (written by ``autotune.py``).
+    """
+
+    def __init__(self, params_list, conf_counts, device=None, bins=DEFAULT_BINS, tuning=None):
+        super().__init__(params_list, conf_counts, device)
+        torch = _torch()
+        n_atoms = np.array([int(p.n_atoms) for p in self.params_list], dtype=np.int64)
+        nconf = n_atoms[self.conf_mol]
+        self.bins = []
+        lo = 0
+        for hi in bins:
+            sel = np.nonzero((nconf > lo) & (nconf <= hi))[0]
+            if len(sel):
+                order = sel[np.lexsort((sel, self.conf_mol[sel], -nconf[sel]))].astype(np.int32)
+                dc = DeviceConformers(self.batch, self.conf_mol, self.conf_coord, order)
+                dc.n_conf = len(order)          # the bin's queue: its own order array
+                dc.max_atoms = int(nconf[sel].max())
+                cfg = dict((tuning or {}).get(str(hi), (tuning or {}).get(hi, {})))
+                self.bins.append({"hi": hi, "confs": dc, "n": len(order), "cfg": cfg,
+                                  "stream": torch.cuda.Stream(device=self.batch.device), "scratch": None,
+                                  "cost": float(np.sum((3.0 * nconf[sel]) ** 2))})
+            lo = hi
+        self.bins.sort(key=lambda b: -b["cost"])
+
+    def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
+                        precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
+                        ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
+                        atom_grad_scale: float = 1.0, stream=None, out=None, evals=None):
+        torch = _torch()
+        L = _lib.load()
+        C = self.confs.n_conf
+        if out is None:
+            e = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+            st = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+            it = torch.empty(C, dtype=torch.int32, device=self.batch.device)
+        else:
+            e, st, it = out
+        main = stream if stream is not None else torch.cuda.current_stream()
+        fork = torch.cuda.Event()
+        fork.record(main)
+        bd = self.batch.desc()
+        for b in self.bins:
+            cfg = b["cfg"]
+            o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode,
+                           threads or cfg.get("threads", 0), ctas_per_sm or cfg.get("ctas_per_sm", 0),
+                           exit_test, check_every, atom_grad_scale)
+            cd = b["confs"].desc()
+            nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
+            if b["scratch"] is None or b["scratch"].numel() < nbytes:
+                b["scratch"] = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.batch.device)
+            s = b["stream"]
+            s.wait_event(fork)
+            rc = L.mmffb_minimize(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), pos_dev.data_ptr(),
+                                  e.data_ptr(), st.data_ptr(), it.data_ptr(),
+                                  evals.data_ptr() if evals is not None else None, b["scratch"].data_ptr(),
+                                  b["scratch"].numel(), ctypes.c_void_p(s.cuda_stream))
+            _lib.check(rc, "mmffb_minimize")
+        for b in self.bins:
+            ev = torch.cuda.Event()
+            ev.record(b["stream"])
+            main.wait_event(ev)
+        return e, st, it
+
+
+def mmff_minimize_nk(
+    mmff_params_list,
+    conf_counts: List[int],
+    positions_3d: np.ndarray,
+    *,
+    max_iters: int = 500,
+    grad_tol: float = 1e-4,
+    use_lbfgs: bool = False,
+) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Minimise N molecules x k conformers on the GPU (one persistent launch).
+
+    Same signature and return values as the reference
+    (mlxmolkit/mmff_minimize.py:231-346): ``positions_3d`` is the flat
+    float32 coordinate array of all conformers, molecule-major; returns
+    (positions float32 flat, energies float32 (C,), converged bool (C,)).
+    ``use_lbfgs`` selects L-BFGS with 8 history pairs instead of dense BFGS.
+    """
+    m = BinnedMinimizer(mmff_params_list, conf_counts, tuning=load_tuning())
+    r = m.minimize(positions_3d, max_iters=max_iters, grad_tol=grad_tol,
+                   history_m=LBFGS_M if use_lbfgs else 0)
+    return r.positions, r.energies.astype(np.float32), r.converged

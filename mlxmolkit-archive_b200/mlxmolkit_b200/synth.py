@@ -290,13 +290,19 @@ def _attach_sites(sk: _Skeleton, rng: np.random.Generator, exclude_halo=True):
 def generate_molecule(rng: np.random.Generator, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macrocycle: bool = False,
                       max_rotatable: int | None = None, name: str = "",
-                      max_tries: int = 50) -> SynthMol:
-    """Grow one seeded drug-like molecule (explicit H) of heavy_lo..heavy_hi heavy atoms."""
+                      max_tries: int = 50, max_atoms: int | None = None) -> SynthMol:
+    """Grow one seeded drug-like molecule (explicit H) of heavy_lo..heavy_hi heavy atoms.
+
+    Draws that exceed max_rotatable rotatable bonds or max_atoms atoms (with H)
+    are rejected and redrawn.
+    """
     for _ in range(max_tries):
         mol = _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name)
         if mol is None:
             continue
         if max_rotatable is not None and count_rotatable(mol) > max_rotatable:
+            continue
+        if max_atoms is not None and mol.GetNumAtoms() > max_atoms:
             continue
         return mol
     raise RuntimeError("molecule generation failed repeatedly")
@@ -1005,13 +1011,14 @@ class Workload:
 
 def make_one_molecule(seed: int, m: int, k: int, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macro_frac: float = 0.0,
-                      max_rotatable: int | None = None, noise: float = 0.1) -> SynthMol:
+                      max_rotatable: int | None = None, noise: float = 0.1,
+                      max_atoms: int | None = None) -> SynthMol:
     """Molecule m of the seeded stream: its own generator seeded by (seed, m)."""
     rng = np.random.default_rng([seed, m])
     macro = macro_frac > 0 and rng.random() < macro_frac
     mol = generate_molecule(rng, heavy_lo, heavy_hi, max_rings=max_rings,
                             macrocycle=macro, max_rotatable=max_rotatable,
-                            name=f"synth-{seed}-{m}")
+                            name=f"synth-{seed}-{m}", max_atoms=max_atoms)
     for c in embed_conformers(mol, int(k), rng, noise=noise):
         mol.AddConformer(c)
     return mol
@@ -1024,7 +1031,7 @@ def _make_one_star(args):
 def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_hi: int,
                    max_rings: int = 3, macro_frac: float = 0.0,
                    max_rotatable: int | None = None, noise: float = 0.1,
-                   workers: int | None = None):
+                   workers: int | None = None, max_atoms: int | None = None):
     """n_mols seeded molecules, each with k (or k[i]) embedded noisy conformers.
 
     Each molecule has its own generator seeded by (seed, index), so the result
@@ -1033,7 +1040,7 @@ def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_h
     import os
     ks = [int(k[m]) if isinstance(k, (list, tuple, np.ndarray)) else int(k)
           for m in range(n_mols)]
-    jobs = [(seed, m, ks[m], heavy_lo, heavy_hi, max_rings, macro_frac, max_rotatable, noise)
+    jobs = [(seed, m, ks[m], heavy_lo, heavy_hi, max_rings, macro_frac, max_rotatable, noise, max_atoms)
             for m in range(n_mols)]
     if workers is None:
         workers = min(os.cpu_count() or 1, 16) if n_mols >= 64 else 1
@@ -1053,7 +1060,7 @@ def make_workload(config: int, seed: int = 0, scale: float = 1.0) -> Workload:
         mols = make_molecules(n(50), 50, seed, 10, 30)
         return Workload("cfg0-50x50-heavy10-30", mols, ["MMFF94"] * len(mols), 2000, False)
     if config in (1, 2):
-        mols = make_molecules(n(2000), 10, seed, 8, 70)
+        mols = make_molecules(n(2000), 10, seed, 8, 70, max_atoms=150)
         var = ["MMFF94" if i % 2 == 0 else "MMFF94s" for i in range(len(mols))]
         return Workload("cfg1-2000x10-heavy8-70", mols, var, 1000, False)
     if config == 3:

@@ -322,7 +322,7 @@ enum { ST_GRAD = 0, ST_MAXIT = 1, ST_TOLX = 2, ST_SLOPE = 3, ST_NONFINITE = 4, S
 static void scale_grad(double *g, int n, double *scale, const double *K) {
     double s = *scale, mx = 0.0;
     for (int i = 0; i < n; ++i) { g[i] *= s; mx = dmax(mx, fabs(g[i])); }
-    while (mx > K[K_GCAP]) {
+    for (int h = 0; h < 256 && mx > K[K_GCAP]; ++h) {   /* bounded: inf never ends */
         s *= 0.5; mx = 0.0;
         for (int i = 0; i < n; ++i) { g[i] *= 0.5; mx = dmax(mx, fabs(g[i])); }
     }

@@ -1,0 +1,183 @@
+"""CUDA kernels (through the C ABI) against the FP64 oracle and the reference's own numbers."""
+import numpy as np
+import pytest
+
+from helpers import golden_mol, golden_params, small_workload
+from mlxmolkit_b200 import mmff_minimize as mm
+from mlxmolkit_b200.mmff_params import extract_mmff_params
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden_batch(golden, variant="MMFF94"):
+    mols = [golden_mol(golden, mi) for mi in range(int(golden["n_mols"]))]
+    params = [extract_mmff_params(m, mmff_variant=variant) for m in mols]
+    pos = np.concatenate([golden[f"m{mi}_pos"].reshape(-1) for mi in range(len(mols))])
+    return mols, params, [3] * len(mols), pos
+
+
+def _split(params, counts, flat):
+    out, o = [], 0
+    for p, k in zip(params, counts):
+        for _ in range(k):
+            out.append(flat[o: o + 3 * p.n_atoms])
+            o += 3 * p.n_atoms
+    return out
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-5), ("fp32", 1e-4), ("fp64", 1e-11)])
+def test_energy_and_gradient_match_the_oracle(golden, precision, tol):
+    _, params, counts, pos = _golden_batch(golden)
+    m = mm.Minimizer(params, counts)
+    e, g = m.energy_grad(pos, precision=precision)
+    xs, gs = _split(params, counts, pos), _split(params, counts, g)
+    pidx = np.repeat(np.arange(len(params)), counts)
+    for c, (x, gg) in enumerate(zip(xs, gs)):
+        eo, go, _ = oracle.energy_grad(params[pidx[c]], x.astype(np.float32).astype(np.float64))
+        assert abs(e[c] - eo) <= tol * max(1.0, abs(eo)), (c, e[c], eo)
+        gt = 1e-10 if precision == "fp64" else 1e-4
+        assert np.abs(gg - go).max() <= gt * max(1.0, np.abs(go).max()), c
+
+
+def test_mega_mode_energy_matches_the_reference_numpy_energy(golden):
+    """Directly against mmff_energy_vectorized's numbers stored in the fixture."""
+    for variant in ("MMFF94", "MMFF94s"):
+        _, params, counts, pos = _golden_batch(golden, variant)
+        m = mm.Minimizer(params, counts)
+        e, g = m.energy_grad(pos, precision="fp64", mode=mm.MODE_MEGA)
+        ref = np.concatenate([golden[f"m{mi}_{variant}_ref_energy"] for mi in range(len(params))])
+        # the fixture coordinates are float64; the kernel reads float32 positions
+        for c in range(len(ref)):
+            assert abs(e[c] - ref[c]) <= 1e-4 * max(1.0, abs(ref[c])), (variant, c, e[c], ref[c])
+
+
+def test_fp64_minimizer_tracks_the_fp64_oracle(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    pos32 = pos.astype(np.float32)
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos32, max_iters=2000, precision="fp64", consts=mm.RDKIT_CONSTS)
+    _, eo, so, io = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=2000,
+                                    consts=oracle.RDKIT_CONSTS)
+    d = np.abs(r.energies - eo)
+    assert np.mean(d < 1e-3) >= 0.9, d
+    assert np.all(d < 0.5), d
+
+
+def test_mixed_minimizer_reaches_the_fp64_minimum(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    pos32 = pos.astype(np.float32)
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos32, max_iters=2000)
+    _, eo, _, _ = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=4000,
+                                  consts=oracle.RDKIT_CONSTS)
+    d = np.abs(r.energies - eo)
+    assert np.mean(d <= 0.1) >= 0.9, d
+    assert r.converged.all(), r.status
+    # reported energy is the energy of the reported coordinates
+    e2, _ = m.energy_grad(r.positions)
+    assert np.allclose(e2, r.energies, rtol=1e-6, atol=1e-4)
+
+
+def test_results_are_bit_reproducible(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    m = mm.Minimizer(params, counts)
+    a = m.minimize(pos, max_iters=300)
+    b = m.minimize(pos, max_iters=300)
+    assert np.array_equal(a.positions, b.positions)
+    assert np.array_equal(a.energies, b.energies)
+    assert np.array_equal(a.iters, b.iters)
+
+
+def test_raising_the_cap_does_not_change_the_answer(golden):
+    """Per-conformer in-kernel exits: a larger max_iters buys nothing after convergence."""
+    _, params, counts, pos = _golden_batch(golden)
+    m = mm.Minimizer(params, counts)
+    a = m.minimize(pos, max_iters=1000)
+    b = m.minimize(pos, max_iters=4000)
+    done = a.status != 1
+    assert done.mean() > 0.8
+    assert np.array_equal(a.energies[done], b.energies[done])
+    assert np.array_equal(a.iters[done], b.iters[done])
+
+
+def test_max_iters_zero_returns_the_initial_energy(golden):
+    """Like the reference's test_mmff_minimize_nk_initial_energy_matches_mlx_energy."""
+    _, params, counts, pos = _golden_batch(golden)
+    pos32, e_in, conv = mm.mmff_minimize_nk(params, counts, pos.astype(np.float32), max_iters=0)
+    assert e_in.dtype == np.float32 and conv.dtype == bool
+    assert not conv.any()
+    m = mm.Minimizer(params, counts)
+    e_ref, _ = m.energy_grad(pos)
+    np.testing.assert_allclose(e_in, e_ref, rtol=1e-6, atol=1e-3)
+    assert np.array_equal(pos32, pos.astype(np.float32))
+
+
+def test_lbfgs_kernel_matches_the_oracle_lbfgs(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    pos32 = pos.astype(np.float32)
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos32, max_iters=3000, history_m=8, precision="fp64", consts=mm.RDKIT_CONSTS)
+    _, eo, _, _ = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=3000, history_m=8,
+                                  consts=oracle.RDKIT_CONSTS)
+    d = np.abs(r.energies - eo)
+    assert np.mean(d < 1e-3) >= 0.8, d
+    rm = m.minimize(pos32, max_iters=3000, history_m=8)
+    assert np.mean(np.abs(rm.energies - eo) <= 0.1) >= 0.8
+
+
+def test_plain_reference_design_path(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    pos32 = pos.astype(np.float32)
+    m = mm.Minimizer(params, counts)
+    r = m.plain_minimize(pos32, max_iters=2000)
+    _, eo, _, _ = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=4000,
+                                  consts=oracle.RDKIT_CONSTS)
+    assert np.mean(np.abs(r.energies - eo) <= 0.5) >= 0.7, np.abs(r.energies - eo)
+
+
+def _bb_sd_oracle(p, x, iters, max_step, lr):
+    """Restatement of the fused optimizer loop (mmff_metal_kernel.py:863-1073) on the FP64 oracle."""
+    x = x.astype(np.float64).copy()
+    prev_x, prev_g = x.copy(), np.zeros_like(x)
+    alpha, e_prev, e = lr, 1e30, 0.0
+    for it in range(iters):
+        e, g, _ = oracle.energy_grad(p, x, mode=oracle.MODE_MEGA)
+        if it > 0 and e > e_prev + 1.0:
+            x = prev_x.copy()
+            alpha = max(alpha * 0.5, 1e-7)
+            e = e_prev
+            continue
+        if it > 0:
+            s, y = x - prev_x, g - prev_g
+            ss, sy = s @ s, s @ y
+            if sy > 1e-20:
+                alpha = min(max(ss / sy, 1e-6), 0.3)
+        e_prev = e
+        prev_x, prev_g = x.copy(), g.copy()
+        g3 = g.reshape(-1, 3)
+        gn = np.sqrt((g3 * g3).sum(1) + 1e-30)
+        s = np.minimum(max_step / gn, alpha)
+        x = (x.reshape(-1, 3) - s[:, None] * g3).reshape(-1)
+    return x, e
+
+
+def test_fused_steepest_descent_follows_its_restatement(golden):
+    _, params, counts, pos = _golden_batch(golden)
+    sel = [0, 1, 6]
+    ps = [params[i] for i in sel]
+    xs = [golden[f"m{i}_pos"][0].reshape(-1).astype(np.float32) for i in sel]
+    m = mm.Minimizer(ps, [1] * len(sel))
+    xo, eo = m.fused_sd(np.concatenate(xs), max_iters=30, max_step=0.3, grad_lr=0.1)
+    for c, (p, x) in enumerate(zip(ps, xs)):
+        _, e_ref = _bb_sd_oracle(p, x, 30, 0.3, 0.1)
+        assert abs(eo[c] - e_ref) <= 1e-2 * max(1.0, abs(e_ref)), (c, eo[c], e_ref)
+
+
+def test_workload_mixture_of_sizes_and_variants():
+    mols, params, counts, pos = small_workload(n_mols=8, k=2, seed=9, lo=8, hi=40, variant="MMFF94s")
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos.astype(np.float32), max_iters=1000)
+    _, eo, _, _ = oracle.minimize(params, counts, pos.astype(np.float32).astype(np.float64),
+                                  max_iters=3000, consts=oracle.RDKIT_CONSTS)
+    assert np.mean(np.abs(r.energies - eo) <= 0.1) >= 0.85, np.abs(r.energies - eo)
