@@ -94,6 +94,12 @@ typedef struct {
     int32_t exit_test;           /* MMFFB_EXIT_* */
     int32_t check_every;         /* MMFFB_EXIT_ATOM_NORM: test every k-th iteration (0 = every) */
     float atom_grad_scale;       /* MMFFB_EXIT_ATOM_NORM: factor on the raw gradient */
+    int32_t max_restarts;        /* 0: exit on a failed line search or an uphill direction, like the
+                                    reference; > 0: reset the inverse Hessian (or L-BFGS history) to the
+                                    identity and continue, at most this many times per conformer */
+    int32_t polish64;            /* MMFFB_PREC_MIXED: when the FP32 line-search energies stall (no
+                                    Armijo decrease or a step below TOLX), continue with FP64 term
+                                    energies of the same FP32 coordinates for the line search */
 } MMFFOptParams;
 
 /* convergence test of mmffb_minimize */

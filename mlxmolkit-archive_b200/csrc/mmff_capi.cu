@@ -183,6 +183,8 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
     P.exit_test = opt->exit_test;
     P.check_every = opt->check_every;
     P.atom_grad_scale = opt->atom_grad_scale;
+    P.max_restarts = opt->max_restarts < 0 ? 0 : opt->max_restarts;
+    P.polish64 = opt->precision == MMFFB_PREC_MIXED && opt->polish64 != 0;
     P.ls_evals = ls_evals;
     P.nmax = confs->max_atoms;
     P.pos = pos;

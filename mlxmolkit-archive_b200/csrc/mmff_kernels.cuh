@@ -80,6 +80,8 @@ struct Params {
     int exit_test;
     int check_every;
     float atom_grad_scale;
+    int max_restarts;
+    int polish64;      // mixed precision: FP64 line-search energies once the FP32 ones stall
     int32_t *ls_evals;
     int nmax;          // largest atom count of the launch (shared-memory layout)
     float *pos;
@@ -95,7 +97,7 @@ __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(
 
 // Shared-memory layout of one CTA (byte offsets).
 struct Layout {
-    size_t pos4, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, red, rho, alpha, mat, total;
+    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, red, rho, alpha, mat, total;
 };
 
 __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, bool mat_in_smem,
@@ -104,6 +106,7 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
     size_t o = 0;
     L.pos4 = o; o = al16(o + 4 * (size_t)nmax * rs);
+    L.pos4d = o; o = al16(o + (rs == 4 ? 4 * (size_t)nmax * 8 : 0));   // FP64 copy (mixed precision)
     L.x = o; o = al16(o + nv * rs);
     L.g = o; o = al16(o + nv * rs);
     L.dir = o; o = al16(o + nv * rs);
@@ -344,6 +347,8 @@ struct Opt {
     static constexpr int NW = NT / 32;
     const Params &P;
     R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *gbuf, *mat;
+    double *pos4d;     // FP64 copy of pos4 (float R only)
+    bool use64;        // line-search energies in FP64 (escalated)
     int *cls;
     double *qa;
     A *red, *rho_s, *alpha_s;
@@ -354,6 +359,8 @@ struct Opt {
     __device__ Opt(const Params &p, unsigned char *sm) : P(p), rsel(0) {
         Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A));
         pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
+        pos4d = (double *)(sm + L.pos4d);
+        use64 = false;
         xo = (R *)(sm + L.xo); dg = (R *)(sm + L.dg); hp = (R *)(sm + L.hp); hq = (R *)(sm + L.hq);
         pxi = (R *)(sm + L.pxi); pc = (R *)(sm + L.pc); pr = (R *)(sm + L.pr); gbuf = (R *)(sm + L.gbuf);
         cls = (int *)(sm + L.cls); qa = (double *)(sm + L.q); red = (A *)(sm + L.red);
@@ -374,7 +381,11 @@ struct Opt {
     }
 
     __device__ __forceinline__ A energy() {
-        A e[1] = {eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv)};
+        A e[1];
+        if (sizeof(R) == 4 && use64)
+            e[0] = (A)eval_terms<double, double, NW, false>(P, m, pos4d, (double *)nullptr, cls, qa, nv);
+        else
+            e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv);
         A z[1] = {A(0)};
         reduce<1, 1>(e, z);
         return e[0];
@@ -392,7 +403,11 @@ struct Opt {
         }
     }
 
-    __device__ __forceinline__ void setpos(int k, R v) { pos4[4 * (k / 3) + (k % 3)] = v; }
+    __device__ __forceinline__ void setpos(int k, R v) {
+        const int o = 4 * (k / 3) + (k % 3);
+        pos4[o] = v;
+        if (sizeof(R) == 4) pos4d[o] = (double)v;
+    }
 
     // One pass over the dense inverse Hessian: apply the pending rank-2 update
     // H_ij += pxi_j*pr_i + pxi_i*pc_j, store, and form hp = H g, hq = H dg.
@@ -474,6 +489,16 @@ struct Opt {
         for (int k = threadIdx.x; k < n; k += NT) dir[k] = -hq[k];
     }
 
+    // inverse Hessian back to the identity (dense) / history cleared (L-BFGS)
+    __device__ __forceinline__ void reset_matrix() {
+        if (!LB) {
+            for (size_t e = threadIdx.x; e < (size_t)n * n; e += NT) {
+                const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
+                mat[e] = i == j ? R(1) : R(0);
+            }
+        }
+    }
+
     __device__ void run(int conf) {
         const int tid = threadIdx.x;
         const KConst &K = P.K;
@@ -481,6 +506,7 @@ struct Opt {
         N = m.n;
         n = 3 * N;
         nv = (3 * P.nmax + 3) & ~3;
+        use64 = false;
         const float *gp = P.pos + P.c.conf_coord[conf];
         for (int k = tid; k < n; k += NT) {
             R v = (R)gp[k];
@@ -523,7 +549,8 @@ struct Opt {
         A E = energy();
         const A max_step = (A)K.maxstep * (sqrt(gs_[1]) > (A)n ? sqrt(gs_[1]) : (A)n);
         int status = MMFFB_ST_MAXIT;
-        int it = 0, done_iters = 0, nevals = 0;
+        int it = 0, done_iters = 0, nevals = 0, restarts = 0;
+        bool fresh = true;     // direction is -g (start or just after a restart)
         bool pending = false;
         int hcount = 0, hidx = 0;
         if (!isfinite((double)E) || !isfinite((double)gs_[0])) {
@@ -558,7 +585,22 @@ struct Opt {
                     m3[0] = m4[0];
                 }
                 const A slope = s3[1];
-                if (!(slope < A(0))) { status = MMFFB_ST_SLOPE; break; }
+                if (!(slope < A(0))) {
+                    if (!fresh && restarts < P.max_restarts) {
+                        // uphill quasi-Newton direction: restart from steepest descent
+                        ++restarts;
+                        fresh = true;
+                        pending = false;
+                        hcount = 0;
+                        hidx = 0;
+                        reset_matrix();
+                        for (int k = tid; k < n; k += NT) dir[k] = -g[k];
+                        __syncthreads();
+                        continue;
+                    }
+                    status = MMFFB_ST_SLOPE;
+                    break;
+                }
                 const A lam_min = (A)K.movetol / (m3[0] > A(1e-30) ? m3[0] : A(1e-30));
 
                 // backtracking line search (tg.metal:192-256)
@@ -604,8 +646,29 @@ struct Opt {
                         x[k] = xo[k];
                         setpos(k, xo[k]);
                     }
+                    if (sizeof(R) == 4 && P.polish64 && !use64) {
+                        // FP32 term energies are at their noise floor: continue with FP64
+                        // line-search energies of the same FP32 coordinates
+                        use64 = true;
+                        __syncthreads();
+                        E = energy();
+                        continue;
+                    }
+                    if (!fresh && restarts < P.max_restarts) {
+                        // no decrease along the quasi-Newton direction: restart from -g
+                        ++restarts;
+                        fresh = true;
+                        pending = false;
+                        hcount = 0;
+                        hidx = 0;
+                        reset_matrix();
+                        for (int k = tid; k < n; k += NT) dir[k] = -g[k];
+                        __syncthreads();
+                        continue;
+                    }
                     __syncthreads();
                 }
+                fresh = false;
                 // xi = x - xold, TOLX (kept per thread until the next reduction)
                 A tolx = A(0);
                 for (int k = tid; k < n; k += NT) {
@@ -639,7 +702,15 @@ struct Opt {
                 reduce<1, 4>(gs2, gm2);
                 if (!isfinite((double)gs2[0]) || !isfinite((double)E)) { status = MMFFB_ST_NONFINITE; break; }
                 if (atom_test && gm2[3] * (A)P.atom_grad_scale <= (A)P.grad_tol) { status = MMFFB_ST_GRAD; break; }
-                if (gm2[2] < (A)K.tolx) { status = ok ? MMFFB_ST_TOLX : MMFFB_ST_LSFAIL; break; }
+                if (gm2[2] < (A)K.tolx) {
+                    if (sizeof(R) == 4 && P.polish64 && !use64) {
+                        use64 = true;
+                        E = energy();
+                    } else {
+                        status = ok ? MMFFB_ST_TOLX : MMFFB_ST_LSFAIL;
+                        break;
+                    }
+                }
                 {
                     R mx = (R)gm2[0] * gsc;
                     for (int h = 0; h < 256 && mx > (R)K.gcap; ++h) { mx *= R(0.5); gsc *= R(0.5); }

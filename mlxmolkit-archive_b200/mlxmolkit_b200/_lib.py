@@ -38,7 +38,8 @@ class MMFFOptParams(ctypes.Structure):
                 ("ctas_per_sm", ctypes.c_int32), ("grad_tol", ctypes.c_float),
                 ("consts", ctypes.c_double * 8), ("mode", ctypes.c_double * 4),
                 ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
-                ("atom_grad_scale", ctypes.c_float)]
+                ("atom_grad_scale", ctypes.c_float), ("max_restarts", ctypes.c_int32),
+                ("polish64", ctypes.c_int32)]
 
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",

@@ -45,10 +45,27 @@ import numpy as np
 
 
 class _Hyb:
-    __slots__ = ("name",)
+    """Hybridization value; one instance per name, also across pickling (worker processes)."""
 
-    def __init__(self, name: str):
-        self.name = name
+    __slots__ = ("name",)
+    _by_name: dict = {}
+
+    def __new__(cls, name: str):
+        inst = cls._by_name.get(name)
+        if inst is None:
+            inst = object.__new__(cls)
+            inst.name = name
+            cls._by_name[name] = inst
+        return inst
+
+    def __reduce__(self):
+        return (_Hyb, (self.name,))
+
+    def __eq__(self, other) -> bool:
+        return isinstance(other, _Hyb) and other.name == self.name
+
+    def __hash__(self) -> int:
+        return hash(self.name)
 
     def __repr__(self) -> str:
         return self.name
@@ -592,9 +609,9 @@ class SynthMMFFProperties:
         same_ring = (m.ring_of[j] >= 0 and m.ring_of[i] == m.ring_of[j] == m.ring_of[k])
         rs = m.ring_size[j]
         nh = int(_is_h(m.types[i])) + int(_is_h(m.types[k]))
-        if h is HybridizationType.SP:
+        if h == HybridizationType.SP:
             return 180.0, 0.32
-        if h is HybridizationType.SP2:
+        if h == HybridizationType.SP2:
             if same_ring:
                 t0 = 120.0 if rs == 6 else 108.0
                 if tj == "NAR":
@@ -628,7 +645,7 @@ class SynthMMFFProperties:
 
     def GetMMFFStretchBendParams(self, mol, i: int, j: int, k: int):
         m = self.mol
-        if m.hyb[j] is HybridizationType.SP:
+        if m.hyb[j] == HybridizationType.SP:
             return None
         def side(t: str) -> float:
             if _is_h(t):
@@ -649,7 +666,7 @@ class SynthMMFFProperties:
     def GetMMFFTorsionParams(self, mol, i: int, j: int, k: int, l: int):
         m = self.mol
         tj, tk = m.types[j], m.types[k]
-        if m.hyb[j] is HybridizationType.SP or m.hyb[k] is HybridizationType.SP:
+        if m.hyb[j] == HybridizationType.SP or m.hyb[k] == HybridizationType.SP:
             return None
         o = m.border[(j, k)]
         ends_h = int(_is_h(m.types[i])) + int(_is_h(m.types[l]))
@@ -738,12 +755,12 @@ def _new_dirs(hyb, existing, n_new, rng, k):
     m = len(existing)
     if n_new <= 0:
         return []
-    if hyb is HybridizationType.SP:
+    if hyb == HybridizationType.SP:
         if m == 0:
             u = _rand_unit(rng, k)
             return [u, -u][:n_new]
         return [-existing[0]][:n_new]
-    if hyb is HybridizationType.SP2:
+    if hyb == HybridizationType.SP2:
         if m == 0:
             u1 = _rand_unit(rng, k)
             p = _rand_perp(u1, rng)
@@ -1047,9 +1064,15 @@ def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_h
     if workers <= 1:
         return [_make_one_star(j) for j in jobs]
     import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(workers) as pool:
-        return pool.map(_make_one_star, jobs, chunksize=max(1, n_mols // (workers * 8)))
+    from concurrent.futures import ProcessPoolExecutor
+    from concurrent.futures.process import BrokenProcessPool
+    try:
+        # spawned workers (never forked: the caller may already hold a CUDA context); a pool
+        # whose workers cannot start (e.g. a __main__ read from stdin) fails fast
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_make_one_star, jobs, chunksize=max(1, n_mols // (workers * 8))))
+    except BrokenProcessPool:
+        return [_make_one_star(j) for j in jobs]
 
 
 def make_workload(config: int, seed: int = 0, scale: float = 1.0) -> Workload:

@@ -313,7 +313,7 @@ static double eval(const Mol *m, const double *x, double *g, double *terms) {
 }
 
 /* ---- optimizer constants (index order shared with the Python wrapper) ---- */
-enum { K_TOLX, K_FUNCTOL, K_MOVETOL, K_EPS, K_MAXSTEP, K_MAXLS, K_GSCALE, K_GCAP };
+enum { K_TOLX, K_FUNCTOL, K_MOVETOL, K_EPS, K_MAXSTEP, K_MAXLS, K_GSCALE, K_GCAP, K_RESTARTS };
 
 /* exit codes; 0 and the converged codes map to the reference's status 0 */
 enum { ST_GRAD = 0, ST_MAXIT = 1, ST_TOLX = 2, ST_SLOPE = 3, ST_NONFINITE = 4, ST_LSFAIL = 5 };
@@ -392,7 +392,8 @@ static int minimize_one(const Mol *m, double *x, int max_iters, double grad_tol,
     double ss = 0.0;
     for (int i = 0; i < n; ++i) ss += x[i] * x[i];
     double max_step = K[K_MAXSTEP] * dmax(sqrt(ss), (double)n);
-    int status = ST_MAXIT, it = 0, hcount = 0, hidx = 0;
+    int status = ST_MAXIT, it = 0, hcount = 0, hidx = 0, restarts = 0, fresh = 1;
+    int max_restarts = (int)K[K_RESTARTS];
     if (!isfinite(E) || !finite_vec(g, n)) { status = ST_NONFINITE; max_iters = 0; }
     for (it = 0; it < max_iters; ++it) {
         memcpy(xold, x, sizeof(double) * n);
@@ -402,11 +403,27 @@ static int minimize_one(const Mol *m, double *x, int max_iters, double grad_tol,
         if (dn > max_step) { double sc = max_step / dn; for (int i = 0; i < n; ++i) dir[i] *= sc; }
         double slope = 0.0;
         for (int i = 0; i < n; ++i) slope += dir[i] * g[i];
-        if (slope >= 0.0) { status = ST_SLOPE; break; }
+        if (slope >= 0.0) {
+            if (!fresh && restarts < max_restarts) {       /* restart from steepest descent */
+                ++restarts; fresh = 1; hcount = 0; hidx = 0;
+                if (hm == 0) for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) H[(size_t)i*n + j] = i == j;
+                for (int i = 0; i < n; ++i) dir[i] = -g[i];
+                continue;
+            }
+            status = ST_SLOPE;
+            break;
+        }
         double tm = 0.0;
         for (int i = 0; i < n; ++i) tm = dmax(tm, fabs(dir[i]) / dmax(fabs(x[i]), 1.0));
         double lam_min = K[K_MOVETOL] / dmax(tm, 1e-30);
         int ok = line_search(m, x, xold, dir, n, Eold, slope, lam_min, &E, K);
+        if (!ok && !fresh && restarts < max_restarts) {    /* x already restored: restart */
+            ++restarts; fresh = 1; hcount = 0; hidx = 0;
+            if (hm == 0) for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) H[(size_t)i*n + j] = i == j;
+            for (int i = 0; i < n; ++i) dir[i] = -g[i];
+            continue;
+        }
+        fresh = 0;
         for (int i = 0; i < n; ++i) xold[i] = x[i] - xold[i];       /* xi */
         double tx = 0.0;
         for (int i = 0; i < n; ++i) tx = dmax(tx, fabs(xold[i]) / dmax(fabs(x[i]), 1.0));

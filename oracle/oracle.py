@@ -100,7 +100,7 @@ def energy_grad(p, x, mode=MODE_TG, want_grad: bool = True):
 
 def minimize(params_list, conf_counts, x_flat, *, max_iters: int, grad_tol: float = 1e-4,
              history_m: int = 0, consts=TG_CONSTS, mode=MODE_TG,
-             n_threads: int = 0, conf_mol=None):
+             n_threads: int = 0, conf_mol=None, max_restarts: int = 0):
     """FP64 BFGS (history_m == 0) or L-BFGS minimisation of every conformer.
 
     Returns (x_out float64 flat, energy (C,), status (C,), iters (C,)).
@@ -128,7 +128,7 @@ def minimize(params_list, conf_counts, x_flat, *, max_iters: int, grad_tol: floa
     status = np.zeros(C, np.int32)
     energy = np.zeros(C, np.float64)
     iters = np.zeros(C, np.int32)
-    K = np.asarray(consts, dtype=np.float64)
+    K = np.concatenate([np.asarray(consts, dtype=np.float64)[:8], [float(max_restarts)]])
     md = np.ascontiguousarray(mode, dtype=np.float64)
     lib().oracle_minimize_batch(M, _p(counts), _p(idx_off), _p(par_off), _p(idx), _p(par), _p(diel),
                                 C, _p(conf_mol), _p(atom_off), _p(x), int(max_iters), float(grad_tol),

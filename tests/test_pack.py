@@ -131,3 +131,17 @@ def test_batch_offsets_are_consistent():
     masks = 2 * pb.n_atoms * W
     assert pb.mol_desc[:, pack.MD_MASK_OFF].tolist() == np.concatenate([[0], np.cumsum(masks)[:-1]]).tolist()
     assert len(pb.pair_mask) == masks.sum()
+
+
+def test_hybridization_survives_pickling_and_worker_pools():
+    """Molecules built in spawned workers must type exactly like serially built ones."""
+    import pickle
+    from mlxmolkit_b200 import synth
+    assert pickle.loads(pickle.dumps(synth.HybridizationType.SP)) is synth.HybridizationType.SP
+    a = synth.make_molecules(6, 1, 21, 8, 40, workers=2)
+    b = synth.make_molecules(6, 1, 21, 8, 40, workers=1)
+    for x, y in zip(a, b):
+        pa, pb = extract_mmff_params(x), extract_mmff_params(y)
+        assert np.array_equal(pa.torsion_idx1, pb.torsion_idx1)
+        assert np.array_equal(pa.strbend_idx2, pb.strbend_idx2)
+        assert np.array_equal(x.GetConformer(0).pos, y.GetConformer(0).pos)
