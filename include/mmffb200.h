@@ -66,6 +66,7 @@ enum {
 typedef struct {
     int32_t n_mols;
     int32_t max_atoms;           /* largest N in the batch */
+    int32_t max_classes;         /* largest per-molecule class count (<= 64) */
     const int32_t *mol_desc;
     const void *bonded;          /* 16-byte aligned records */
     const int32_t *atom_cls;
@@ -86,7 +87,7 @@ typedef struct {
     int32_t max_iters;
     int32_t history_m;           /* 0: dense BFGS; > 0: L-BFGS with that many pairs */
     int32_t precision;           /* MMFFB_PREC_* */
-    int32_t threads;             /* CTA size 64, 128 or 256; 0 = choose from max_atoms */
+    int32_t threads;             /* CTA size 64, 128, 256 or 512 (512: streamed H only); 0 = auto */
     int32_t ctas_per_sm;         /* persistent CTAs per SM; 0 = as many as fit */
     float grad_tol;
     double consts[8];            /* TOLX FUNCTOL MOVETOL EPS MAXSTEP_FACTOR MAX_LS GRAD_SCALE GRAD_CAP */
@@ -100,6 +101,8 @@ typedef struct {
     int32_t polish64;            /* MMFFB_PREC_MIXED: when the FP32 line-search energies stall (no
                                     Armijo decrease or a step below TOLX), continue with FP64 term
                                     energies of the same FP32 coordinates for the line search */
+    int32_t hpass_lean;          /* inverse Hessian in global memory: read its column vectors from
+                                    shared memory instead of registers (2 CTAs per SM) */
 } MMFFOptParams;
 
 /* convergence test of mmffb_minimize */

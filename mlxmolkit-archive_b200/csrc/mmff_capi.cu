@@ -43,6 +43,8 @@ static int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c) {
         return fail(MMFFB_EINVAL, "null device pointer in batch");
     if (c->max_atoms <= 0 && c->n_conf > 0) return fail(MMFFB_EINVAL, "max_atoms must be positive");
     if (c->max_atoms > kMaxAtoms) return fail(MMFFB_ETOOBIG, "molecule of %d atoms exceeds %d", c->max_atoms, kMaxAtoms);
+    if (b->max_classes < 1 || b->max_classes > 64)
+        return fail(MMFFB_EINVAL, "max_classes must be in 1..64 (got %d)", b->max_classes);
     return 0;
 }
 
@@ -61,7 +63,7 @@ static KConst to_consts(const double *k) {
 
 // Pick the kernel instance (CTA size, register-cached H columns, matrix in
 // shared or global memory) and the persistent grid for these conformers.
-static int plan_minimize(const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl) {
+static int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl) {
     int sms = 0, optin = 0;
     int r = device_props(&sms, &optin);
     if (r) return r;
@@ -75,21 +77,31 @@ static int plan_minimize(const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl)
     const bool lb = o->history_m > 0;
     int nt = o->threads;
     if (nt == 0) nt = nmax <= 24 ? 64 : (nmax <= 48 ? 128 : 256);
-    if (nt != 64 && nt != 128 && nt != 256) return fail(MMFFB_EINVAL, "threads must be 64, 128 or 256");
+    if (nt != 64 && nt != 128 && nt != 256 && nt != 512)
+        return fail(MMFFB_EINVAL, "threads must be 64, 128, 256 or 512");
     if (!mixed || lb) nt = 256;
     if (!lb && n > 512) return fail(MMFFB_ETOOBIG, "dense BFGS supports up to 170 atoms (got %d); use L-BFGS", nmax);
-    Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as);
+    const int mc = b->max_classes;
+    if (nt == 512 && (lb || !mixed)) nt = 256;
+    Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as, mc);
     bool msm = Ls.total <= (size_t)optin;
     int nc = 2;
     if (!lb) {
         if (msm) {
+            if (nt == 512) nt = 256;
             if (nt == 64 && n > 128) nt = 128;
             nc = nt == 64 ? 4 : 8;
             if (n > 32 * nc) msm = false;
         }
-        if (!msm) { nt = 256; nc = 16; }
+        if (!msm) {
+            // streamed H: register-cached columns (1 CTA/SM), or the register-lean form
+            // (columns from shared memory) at 2 CTAs/SM (256 threads) or 512 threads
+            const bool lean = mixed && (o->hpass_lean || nt == 512);
+            if (nt != 512) nt = 256;
+            nc = lean ? 0 : 16;
+        }
     }
-    Layout L = make_layout(nmax, nt / 32, o->history_m, msm, rs, as);
+    Layout L = make_layout(nmax, nt / 32, o->history_m, msm, rs, as, mc);
     if (L.total > (size_t)optin)
         return fail(MMFFB_ETOOBIG, "molecule of %d atoms needs %zu B of shared memory", nmax, L.total);
     pl->nt = nt;
@@ -145,7 +157,7 @@ size_t mmffb_minimize_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev
                                     const MMFFOptParams *opt) {
     if (check_batch(batch, confs) || !opt) return 0;
     Plan pl;
-    if (plan_minimize(confs, opt, &pl)) return 0;
+    if (plan_minimize(batch, confs, opt, &pl)) return 0;
     size_t b = 256;
     if (!pl.msm) b += (size_t)pl.grid * pl.gslot * pl.rsz;
     return b;
@@ -163,7 +175,7 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
         return fail(MMFFB_EINVAL, "unknown exit_test %d", opt->exit_test);
     if (confs->n_conf == 0) return 0;
     Plan pl;
-    r = plan_minimize(confs, opt, &pl);
+    r = plan_minimize(batch, confs, opt, &pl);
     if (r) return r;
     size_t need = 256 + (pl.msm ? 0 : (size_t)pl.grid * pl.gslot * pl.rsz);
     if (!scratch || scratch_bytes < need)
@@ -192,6 +204,7 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
     P.status = status;
     P.iters = iters;
     P.counter = reinterpret_cast<int *>(scratch);
+    P.err = reinterpret_cast<int *>(scratch) + 1;
     P.gmat = reinterpret_cast<unsigned char *>(scratch) + 256;
     P.gslot = pl.gslot;
     if (opt->precision == MMFFB_PREC_FP64) return minimize_fp64(P, pl, st);

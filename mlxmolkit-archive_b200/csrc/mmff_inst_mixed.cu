@@ -13,7 +13,11 @@ static int with_instance(const Plan &pl, bool lb, const Fn &fn) {
     using A = double;
     if (lb) return pl.msm ? fn.template run<R, A, 256, 2, true, true>()
                           : fn.template run<R, A, 256, 2, false, true>();
-    if (!pl.msm) return fn.template run<R, A, 256, 16, false, false>();
+    if (!pl.msm) {
+        if (pl.nc == 0) return pl.nt == 512 ? fn.template run<R, A, 512, 0, false, false>()
+                                            : fn.template run<R, A, 256, 0, false, false>();
+        return fn.template run<R, A, 256, 16, false, false>();
+    }
     if (pl.nt == 64) return fn.template run<R, A, 64, 4, true, false>();
     if (pl.nt == 128) return fn.template run<R, A, 128, 8, true, false>();
     return fn.template run<R, A, 256, 8, true, false>();

@@ -83,6 +83,7 @@ struct Params {
     int max_restarts;
     int polish64;      // mixed precision: FP64 line-search energies once the FP32 ones stall
     int32_t *ls_evals;
+    int *err;          // set when a bounded wait gave up (never expected)
     int nmax;          // largest atom count of the launch (shared-memory layout)
     float *pos;
     double *energy;
@@ -96,12 +97,18 @@ struct Params {
 __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 // Shared-memory layout of one CTA (byte offsets).
+constexpr int kStages = 4;         // rows of H in flight per warp (TMA ring)
+
 struct Layout {
-    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, red, rho, alpha, mat, total;
+    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, qf, mask, tab, red, rho, alpha,
+        ring, mbar, mat, total;
 };
 
+// row stride of a dense inverse Hessian in global memory: 16-byte multiple for TMA rows
+__host__ __device__ __forceinline__ int hld(int n) { return (n + 3) & ~3; }
+
 __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, bool mat_in_smem,
-                                              size_t rs, size_t as) {
+                                              size_t rs, size_t as, int max_classes = 32) {
     Layout L;
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
     size_t o = 0;
@@ -120,9 +127,19 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
     L.gbuf = o; o = al16(o + (size_t)nwarps * nv * rs);
     L.cls = o; o = al16(o + (size_t)nmax * 4);
     L.q = o; o = al16(o + (size_t)nmax * 8);
+    L.qf = o; o = al16(o + (size_t)nmax * 4);
+    L.mask = o; o = al16(o + 2 * (size_t)nmax * ((nmax + 31) / 32) * 4);
+    L.tab = o; o = al16(o + (size_t)max_classes * max_classes * 8);
     L.red = o; o = al16(o + 2 * (size_t)nwarps * 8 * as);
     L.rho = o; o = al16(o + kMaxHist * as);
     L.alpha = o; o = al16(o + kMaxHist * as);
+    L.ring = o;
+    L.mbar = o;
+    if (!mat_in_smem && hist_m == 0) {             // TMA row ring of the streamed H pass
+        o = al16(o + (size_t)nwarps * kStages * hld(3 * nmax) * rs);
+        L.mbar = o;
+        o = al16(o + (size_t)nwarps * kStages * 8);
+    }
     L.mat = o;
     if (mat_in_smem) {
         size_t me = hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)(3 * nmax);
@@ -134,8 +151,46 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
 
 __host__ __device__ inline size_t mat_elems(int nmax, int hist_m) {
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
-    return hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)(3 * nmax);
+    return hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)hld(3 * nmax);
 }
+
+// ---- TMA bulk copies and mbarriers (inline PTX) ----
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// 1-D bulk copy global -> shared (no multicast), completion counted on the mbarrier
+__device__ __forceinline__ void tma_load_row(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+constexpr uint32_t kMaxWaitSpins = 1u << 22;   // bounded waits: give up, flag, never hang
 
 template <class R> __device__ __forceinline__ R qprod(double a, double b);
 template <> __device__ __forceinline__ float qprod<float>(double a, double b) { return (float)(a * b); }
@@ -192,11 +247,53 @@ template <class R> __device__ __forceinline__ void add3(R *dst, const R *f) {
 
 __device__ __forceinline__ float u2f(uint32_t u) { return __uint_as_float(u); }
 
+// Per-conformer molecule data staged in shared memory.
+struct MolSmem {
+    const int *cls;        // non-bonded class per atom
+    const double *qa;      // partial charge per atom (FP64)
+    const float *qf;       // the same, float (FP32 pair math)
+    const uint32_t *mask;  // N x W non-bonded-pair bit rows, then N x W 1-4 bit rows
+    const float2 *tab;     // ncls x ncls (R*, eps)
+};
+
+template <class R> __device__ __forceinline__ void ld3(const R *p4, int a, R &x, R &y, R &z) {
+    x = p4[4 * a]; y = p4[4 * a + 1]; z = p4[4 * a + 2];
+}
+template <> __device__ __forceinline__ void ld3<float>(const float *p4, int a, float &x, float &y, float &z) {
+    const float4 v = reinterpret_cast<const float4 *>(p4)[a];
+    x = v.x; y = v.y; z = v.z;
+}
+
+template <class R> __device__ __forceinline__ R pair_charge(const MolSmem &ms, int i, int j);
+template <> __device__ __forceinline__ float pair_charge<float>(const MolSmem &ms, int i, int j) {
+    return ms.qf[i] * ms.qf[j];
+}
+template <> __device__ __forceinline__ double pair_charge<double>(const MolSmem &ms, int i, int j) {
+    return qprod<double>(ms.qa[i], ms.qa[j]);
+}
+
+// Copy a molecule's bit rows, class table, classes and charges into shared memory.
+template <int NT>
+__device__ __forceinline__ void stage_molecule(const Params &P, const MolV &m, int *cls, double *qa, float *qf,
+                                               uint32_t *mask, float2 *tab) {
+    const int N = m.n, W = (N + 31) >> 5;
+    for (int a = threadIdx.x; a < N; a += NT) {
+        cls[a] = P.b.atom_cls[m.atom_off + a];
+        const double q = P.b.atom_q[m.atom_off + a];
+        qa[a] = q;
+        qf[a] = (float)q;
+    }
+    const uint32_t *gm = P.b.pair_mask + m.mask_off;
+    for (int k = threadIdx.x; k < 2 * N * W; k += NT) mask[k] = gm[k];
+    const float2 *gt = reinterpret_cast<const float2 *>(P.b.cls_tab) + m.cls_off;
+    for (int k = threadIdx.x; k < m.ncls * m.ncls; k += NT) tab[k] = gt[k];
+}
+
 // Energy (thread partial, not reduced) and -- if G -- per-warp gradient buffers.
-// pos4: smem float4-strided coordinates; gbuf: NW x nv; cls/qa: per atom.
+// pos4: smem float4-strided coordinates; gbuf: NW x nv.
 template <class R, class A, int NW, bool G>
 __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R *pos4, R *gbuf,
-                                        const int *cls, const double *qa, int nv) {
+                                        const MolSmem &ms, int nv) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int N = m.n;
     A acc = A(0);
@@ -296,27 +393,27 @@ __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R 
         }
     }
 
-    // non-bonded pairs, implicit from the bit rows
+    // non-bonded pairs, implicit from the staged bit rows and class table
     const int W = (N + 31) >> 5;
-    const uint32_t *pm = P.b.pair_mask + m.mask_off;
-    const uint32_t *p14 = pm + (size_t)N * W;
-    const float2 *tab = reinterpret_cast<const float2 *>(P.b.cls_tab) + m.cls_off;
+    const uint32_t *pm = ms.mask, *p14 = ms.mask + (size_t)N * W;
     const bool dd = m.diel == 2;
     for (int i = warp; i < N - 1; i += NW) {
-        const R xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
-        const int ci = cls[i] * m.ncls;
-        const double qi = qa[i];
+        R xi, yi, zi;
+        ld3(pos4, i, xi, yi, zi);
+        const int ci = ms.cls[i] * m.ncls;
         R fx = R(0), fy = R(0), fz = R(0);
         for (int jb = (i + 1) & ~31; jb < N; jb += 32) {
-            const uint32_t wd = __ldg(pm + (size_t)i * W + (jb >> 5));
+            const uint32_t wd = pm[i * W + (jb >> 5)];
             if (wd == 0u) continue;
+            const uint32_t w14 = p14[i * W + (jb >> 5)];
             if ((wd >> lane) & 1u) {
                 const int j = jb + lane;
-                const uint32_t w14 = __ldg(p14 + (size_t)i * W + (jb >> 5));
-                const float2 t = __ldg(tab + ci + cls[j]);
-                R qq = qprod<R>(qi, qa[j]);
+                const float2 t = ms.tab[ci + ms.cls[j]];
+                R qq = pair_charge<R>(ms, i, j);
                 if ((w14 >> lane) & 1u) qq *= R(0.75);
-                const R dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+                R xj, yj, zj;
+                ld3(pos4, j, xj, yj, zj);
+                const R dx = xi - xj, dy = yi - yj, dz = zi - zj;
                 R ev, ee, s;
                 pair_term<R, G>(dx, dy, dz, (R)t.x, (R)t.y, qq, dd, ev, ee, s);
                 acc += (A)ev;
@@ -348,22 +445,36 @@ struct Opt {
     const Params &P;
     R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *gbuf, *mat;
     double *pos4d;     // FP64 copy of pos4 (float R only)
+    R *ring;           // TMA row ring (streamed H pass)
+    uint64_t *mbar;    // one mbarrier per ring stage and warp
+    uint32_t phase;    // parity of each of this warp's stages
+    int ldh;           // row stride of H
     bool use64;        // line-search energies in FP64 (escalated)
     int *cls;
     double *qa;
+    float *qf;
+    uint32_t *mask;
+    float2 *tab;
+    MolSmem ms;
     A *red, *rho_s, *alpha_s;
     int rsel;
     MolV m;
     int N, n, nv;
 
     __device__ Opt(const Params &p, unsigned char *sm) : P(p), rsel(0) {
-        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A));
+        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes);
         pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
         pos4d = (double *)(sm + L.pos4d);
         use64 = false;
+        ring = (R *)(sm + L.ring);
+        mbar = (uint64_t *)(sm + L.mbar);
+        phase = 0;
+        ldh = 0;
         xo = (R *)(sm + L.xo); dg = (R *)(sm + L.dg); hp = (R *)(sm + L.hp); hq = (R *)(sm + L.hq);
         pxi = (R *)(sm + L.pxi); pc = (R *)(sm + L.pc); pr = (R *)(sm + L.pr); gbuf = (R *)(sm + L.gbuf);
         cls = (int *)(sm + L.cls); qa = (double *)(sm + L.q); red = (A *)(sm + L.red);
+        qf = (float *)(sm + L.qf); mask = (uint32_t *)(sm + L.mask); tab = (float2 *)(sm + L.tab);
+        ms.cls = cls; ms.qa = qa; ms.qf = qf; ms.mask = mask; ms.tab = tab;
         rho_s = (A *)(sm + L.rho); alpha_s = (A *)(sm + L.alpha);
         if (MSM) mat = (R *)(sm + L.mat);
         else mat = (R *)p.gmat + (size_t)blockIdx.x * p.gslot;
@@ -383,9 +494,9 @@ struct Opt {
     __device__ __forceinline__ A energy() {
         A e[1];
         if (sizeof(R) == 4 && use64)
-            e[0] = (A)eval_terms<double, double, NW, false>(P, m, pos4d, (double *)nullptr, cls, qa, nv);
+            e[0] = (A)eval_terms<double, double, NW, false>(P, m, pos4d, (double *)nullptr, ms, nv);
         else
-            e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv);
+            e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, ms, nv);
         A z[1] = {A(0)};
         reduce<1, 1>(e, z);
         return e[0];
@@ -393,7 +504,7 @@ struct Opt {
 
     // gradient at pos4 into dst (raw, unscaled); needs a preceding __syncthreads after pos4 writes
     __device__ __forceinline__ void gradient(R *dst) {
-        eval_terms<R, A, NW, true>(P, m, pos4, gbuf, cls, qa, nv);
+        eval_terms<R, A, NW, true>(P, m, pos4, gbuf, ms, nv);
         __syncthreads();
         for (int k = threadIdx.x; k < n; k += NT) {
             R s = R(0);
@@ -413,7 +524,8 @@ struct Opt {
     // H_ij += pxi_j*pr_i + pxi_i*pc_j, store, and form hp = H g, hq = H dg.
     __device__ __forceinline__ void hpass(bool pending) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        R cx[NC], cc[NC], cg[NC], cd[NC];
+        constexpr int NCR = NC > 0 ? NC : 1;   // NC == 0: columns read from shared memory
+        R cx[NCR], cc[NCR], cg[NCR], cd[NCR];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
             const int j = lane + 32 * c;
@@ -424,9 +536,21 @@ struct Opt {
             cd[c] = in ? dg[j] : R(0);
         }
         for (int i = warp; i < n; i += NW) {
-            R *row = mat + (size_t)i * n;
+            R *row = mat + (size_t)i * ldh;
             const R ri = pending ? pr[i] : R(0), xi = pending ? pxi[i] : R(0);
             R ap = R(0), aq = R(0);
+            if (NC == 0) {
+                for (int j = lane; j < n; j += 32) {
+                    R h = row[j];
+                    if (pending) {
+                        h = fma(pxi[j], ri, h);
+                        h = fma(xi, pc[j], h);
+                        row[j] = h;
+                    }
+                    ap = fma(h, g[j], ap);
+                    aq = fma(h, dg[j], aq);
+                }
+            }
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 const int j = lane + 32 * c;
@@ -445,6 +569,87 @@ struct Opt {
             aq = wsum(aq);
             if (lane == 0) { hp[i] = ap; hq[i] = aq; }
         }
+    }
+
+    // The same pass with H in global memory: each warp streams its rows through a
+    // kStages-deep shared-memory ring with 1-D TMA bulk copies (completion on one
+    // mbarrier per stage), so kStages rows per warp are in flight while the
+    // previous ones are updated; updated rows go back with coalesced stores.
+    __device__ __forceinline__ void hpass_stream(bool pending) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        constexpr int NCR = NC > 0 ? NC : 1;   // NC == 0: columns read from shared memory
+        R cx[NCR], cc[NCR], cg[NCR], cd[NCR];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int j = lane + 32 * c;
+            const bool in = j < n;
+            cx[c] = in ? pxi[j] : R(0);
+            cc[c] = in ? pc[j] : R(0);
+            cg[c] = in ? g[j] : R(0);
+            cd[c] = in ? dg[j] : R(0);
+        }
+        const int ldr = hld(3 * P.nmax);
+        R *rw = ring + (size_t)warp * kStages * ldr;
+        uint64_t *bw = mbar + warp * kStages;
+        const int nrows = warp < n ? (n - warp + NW - 1) / NW : 0;
+        const uint32_t bytes = (uint32_t)(ldh * sizeof(R));
+        if (lane == 0) {
+            for (int t = 0; t < nrows && t < kStages; ++t) {
+                mbar_expect_tx(&bw[t], bytes);
+                tma_load_row(rw + (size_t)t * ldr, mat + (size_t)(warp + NW * t) * ldh, bytes, &bw[t]);
+            }
+        }
+        for (int t = 0; t < nrows; ++t) {
+            const int st = t % kStages, i = warp + NW * t;
+            uint32_t spins = 0;
+            while (!mbar_try_wait(&bw[st], (phase >> st) & 1u)) {
+                if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
+            }
+            phase ^= 1u << st;
+            const R *src = rw + (size_t)st * ldr;
+            R *row = mat + (size_t)i * ldh;
+            const R ri = pending ? pr[i] : R(0), xi = pending ? pxi[i] : R(0);
+            R ap = R(0), aq = R(0);
+            if (NC == 0) {
+                for (int j = lane; j < n; j += 32) {
+                    R h = src[j];
+                    if (pending) {
+                        h = fma(pxi[j], ri, h);
+                        h = fma(xi, pc[j], h);
+                        row[j] = h;
+                    }
+                    ap = fma(h, g[j], ap);
+                    aq = fma(h, dg[j], aq);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int j = lane + 32 * c;
+                if (j < n) {
+                    R h = src[j];
+                    if (pending) {
+                        h = fma(cx[c], ri, h);
+                        h = fma(xi, cc[c], h);
+                        row[j] = h;
+                    }
+                    ap = fma(h, cg[c], ap);
+                    aq = fma(h, cd[c], aq);
+                }
+            }
+            ap = wsum(ap);   // also orders every lane's reads of this stage before its reuse
+            aq = wsum(aq);
+            if (lane == 0) {
+                hp[i] = ap;
+                hq[i] = aq;
+                if (t + kStages < nrows) {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(&bw[st], bytes);
+                    tma_load_row(rw + (size_t)st * ldr, mat + (size_t)(warp + NW * (t + kStages)) * ldh, bytes,
+                                 &bw[st]);
+                }
+            }
+        }
+        fence_proxy_async_global();   // this pass's row stores before the next pass's TMA reads
     }
 
     // L-BFGS two-loop recursion (lbfgs_tg.metal:264-292): dir = -H g from the ring history
@@ -492,10 +697,11 @@ struct Opt {
     // inverse Hessian back to the identity (dense) / history cleared (L-BFGS)
     __device__ __forceinline__ void reset_matrix() {
         if (!LB) {
-            for (size_t e = threadIdx.x; e < (size_t)n * n; e += NT) {
-                const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
+            for (size_t e = threadIdx.x; e < (size_t)n * ldh; e += NT) {
+                const int i = (int)(e / ldh), j = (int)(e - (size_t)i * ldh);
                 mat[e] = i == j ? R(1) : R(0);
             }
+            if (!MSM) fence_proxy_async_global();
         }
     }
 
@@ -513,16 +719,9 @@ struct Opt {
             x[k] = v;
             setpos(k, v);
         }
-        for (int a = tid; a < N; a += NT) {
-            cls[a] = P.b.atom_cls[m.atom_off + a];
-            qa[a] = P.b.atom_q[m.atom_off + a];
-        }
-        if (!LB) {
-            for (size_t e = tid; e < (size_t)n * n; e += NT) {
-                const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
-                mat[e] = i == j ? R(1) : R(0);
-            }
-        }
+        stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
+        ldh = MSM ? n : hld(n);
+        if (!LB) reset_matrix();
         __syncthreads();
 
         // initial gradient and scale (header :435-454, tg.metal:115-122)
@@ -728,7 +927,8 @@ struct Opt {
                 }
                 if (!LB) {
                     __syncthreads();
-                    hpass(pending);
+                    if (MSM) hpass(pending);
+                    else hpass_stream(pending);
                     __syncthreads();
                     A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};
                     for (int k = tid; k < n; k += NT) {
@@ -794,10 +994,17 @@ struct Opt {
 };
 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>
-__global__ void __launch_bounds__(NT) minimize_kernel(const Params P) {
+__global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_kernel(const Params P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     Opt<R, A, NT, NC, MSM, LB> opt(P, smem);
+    if (!MSM && !LB) {
+        if (threadIdx.x == 0) {
+            for (int b = 0; b < (NT / 32) * kStages; ++b) mbar_init(&opt.mbar[b], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
     const int *order = P.c.order;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
@@ -818,23 +1025,24 @@ __global__ void __launch_bounds__(NT) energy_grad_kernel(const Params P, float *
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int NW = NT / 32;
     const int conf = blockIdx.x;
-    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A));
+    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A), P.b.max_classes);
     R *pos4 = (R *)(smem + L.pos4), *gbuf = (R *)(smem + L.gbuf);
     int *cls = (int *)(smem + L.cls);
     double *qa = (double *)(smem + L.q);
+    float *qf = (float *)(smem + L.qf);
+    uint32_t *mask = (uint32_t *)(smem + L.mask);
+    float2 *tab = (float2 *)(smem + L.tab);
     A *red = (A *)(smem + L.red);
     const MolV m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
     const int n = 3 * m.n, nv = (3 * P.nmax + 3) & ~3;
     const float *gp = P.pos + P.c.conf_coord[conf];
     for (int k = threadIdx.x; k < n; k += NT) pos4[4 * (k / 3) + (k % 3)] = (R)gp[k];
-    for (int a = threadIdx.x; a < m.n; a += NT) {
-        cls[a] = P.b.atom_cls[m.atom_off + a];
-        qa[a] = P.b.atom_q[m.atom_off + a];
-    }
+    stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
+    const MolSmem ms{cls, qa, qf, mask, tab};
     __syncthreads();
     A e[1], z[1] = {A(0)};
-    if (grad) e[0] = eval_terms<R, A, NW, true>(P, m, pos4, gbuf, cls, qa, nv);
-    else e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, cls, qa, nv);
+    if (grad) e[0] = eval_terms<R, A, NW, true>(P, m, pos4, gbuf, ms, nv);
+    else e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, ms, nv);
     block_reduce<NW, 1, 1, A>(e, z, red);
     if (grad) {
         float *go = grad + P.c.conf_coord[conf];
@@ -871,7 +1079,7 @@ int launch_min(const Params &P, const Plan &pl, cudaStream_t st) {
 
 template <class R, class A, int NT>
 int launch_eg(const Params &P, float *grad, cudaStream_t st) {
-    Layout L = make_layout(P.nmax, NT / 32, 0, false, sizeof(R), sizeof(A));
+    Layout L = make_layout(P.nmax, NT / 32, 0, false, sizeof(R), sizeof(A), P.b.max_classes);
     auto k = energy_grad_kernel<R, A, NT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");

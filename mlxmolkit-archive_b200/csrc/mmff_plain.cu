@@ -320,11 +320,14 @@ __global__ void __launch_bounds__(NT) fused_sd_kernel(const Params P, float max_
     using R = float;
     using A = double;
     const int conf = blockIdx.x, tid = threadIdx.x;
-    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A));
+    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A), P.b.max_classes);
     R *pos4 = (R *)(smem + L.pos4), *x = (R *)(smem + L.x), *g = (R *)(smem + L.g);
     R *pp = (R *)(smem + L.xo), *pg = (R *)(smem + L.dg), *gbuf = (R *)(smem + L.gbuf);
     int *cls = (int *)(smem + L.cls);
     double *qa = (double *)(smem + L.q);
+    float *qf = (float *)(smem + L.qf);
+    uint32_t *mask = (uint32_t *)(smem + L.mask);
+    float2 *tab = (float2 *)(smem + L.tab);
     A *red = (A *)(smem + L.red);
     int rsel = 0;
     const MolV m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
@@ -335,15 +338,13 @@ __global__ void __launch_bounds__(NT) fused_sd_kernel(const Params P, float max_
         x[k] = v; pp[k] = v; pg[k] = R(0);
         pos4[4 * (k / 3) + (k % 3)] = v;
     }
-    for (int a = tid; a < N; a += NT) {
-        cls[a] = P.b.atom_cls[m.atom_off + a];
-        qa[a] = P.b.atom_q[m.atom_off + a];
-    }
+    stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
+    const MolSmem ms{cls, qa, qf, mask, tab};
     __syncthreads();
     R alpha = grad_lr;
     A E = A(0), Eprev = A(1e30);
     for (int it = 0; it < P.max_iters; ++it) {
-        A e1[1] = {eval_terms<R, A, NW, true>(P, m, pos4, gbuf, cls, qa, nv)}, z[1] = {A(0)};
+        A e1[1] = {eval_terms<R, A, NW, true>(P, m, pos4, gbuf, ms, nv)}, z[1] = {A(0)};
         __syncthreads();
         for (int k = tid; k < n; k += NT) {
             R s = R(0);
@@ -397,6 +398,7 @@ static int check_common(const MMFFBatchDev *b, const MMFFConfDev *c) {
         return fail(MMFFB_EINVAL, "null device pointer in batch");
     if (c->n_conf > 0 && (c->max_atoms <= 0 || c->max_atoms > 1024))
         return fail(MMFFB_EINVAL, "max_atoms out of range");
+    if (b->max_classes < 1 || b->max_classes > 64) return fail(MMFFB_EINVAL, "max_classes out of range");
     return 0;
 }
 
@@ -467,7 +469,7 @@ int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
     P.pos = pos;
     P.energy = energy;
     constexpr int NT = 128;
-    Layout L = make_layout(P.nmax, NT / 32, 0, false, 4, 8);
+    Layout L = make_layout(P.nmax, NT / 32, 0, false, 4, 8, batch->max_classes);
     auto k = fused_sd_kernel<NT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");

@@ -22,10 +22,13 @@ struct TermMode {
 };
 
 template <class R> struct Num;
+// FP32: hardware approximate reciprocal / reciprocal square root (about 2 ulp); the
+// FP32 paths are checked against the FP64 oracle to 1e-5 relative, and the line
+// search of the mixed path switches to FP64 energies near convergence.
 template <> struct Num<float> {
-    static __device__ __forceinline__ float sqrt_(float x) { return __fsqrt_rn(x); }
-    static __device__ __forceinline__ float rsqrt_(float x) { return __frsqrt_rn(x); }
-    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return x * rsqrtf(x); }   // x > 0 here
+    static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
     static __device__ __forceinline__ float acos_(float x) { return acosf(x); }
     static __device__ __forceinline__ float asin_(float x) { return asinf(x); }
 };

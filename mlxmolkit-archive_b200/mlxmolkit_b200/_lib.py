@@ -22,7 +22,7 @@ EXIT_TG, EXIT_ATOM_NORM = 0, 1
 
 
 class MMFFBatchDev(ctypes.Structure):
-    _fields_ = [("n_mols", ctypes.c_int32), ("max_atoms", ctypes.c_int32),
+    _fields_ = [("n_mols", ctypes.c_int32), ("max_atoms", ctypes.c_int32), ("max_classes", ctypes.c_int32),
                 ("mol_desc", P), ("bonded", P), ("atom_cls", P), ("atom_q", P),
                 ("cls_tab", P), ("pair_mask", P)]
 
@@ -39,7 +39,7 @@ class MMFFOptParams(ctypes.Structure):
                 ("consts", ctypes.c_double * 8), ("mode", ctypes.c_double * 4),
                 ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
                 ("atom_grad_scale", ctypes.c_float), ("max_restarts", ctypes.c_int32),
-                ("polish64", ctypes.c_int32)]
+                ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32)]
 
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",

@@ -79,7 +79,8 @@ class DeviceBatch:
         return cls(pack_molecules(params_list), device)
 
     def desc(self) -> _lib.MMFFBatchDev:
-        return _lib.MMFFBatchDev(self.packed.n_mols, self.packed.max_atoms, self.mol_desc.data_ptr(),
+        return _lib.MMFFBatchDev(self.packed.n_mols, self.packed.max_atoms, self.packed.max_classes,
+                                 self.mol_desc.data_ptr(),
                                  self.bonded.data_ptr(), self.atom_cls.data_ptr(), self.atom_q.data_ptr(),
                                  self.cls_tab.data_ptr(), self.pair_mask.data_ptr())
 
@@ -107,12 +108,13 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                consts=TG_CONSTS, mode=MODE_TG, threads: int = 0, ctas_per_sm: int = 0,
                exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
-               polish64: Optional[bool] = None) -> _lib.MMFFOptParams:
+               polish64: Optional[bool] = None, hpass_lean: bool = True) -> _lib.MMFFOptParams:
     """Launch options; ``polish64`` (default: on for mixed precision) switches a conformer's
     line-search energies to FP64 once the FP32 ones stall."""
     o = _lib.MMFFOptParams()
     o.max_restarts = int(max_restarts)
     o.polish64 = int(precision == "mixed" if polish64 is None else bool(polish64))
+    o.hpass_lean = int(bool(hpass_lean))
     o.exit_test = int(exit_test)
     o.check_every = int(check_every)
     o.atom_grad_scale = float(atom_grad_scale)
@@ -168,8 +170,8 @@ class Minimizer:
     def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
-                        atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None, stream=None,
-                        out=None, evals=None):
+                        atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
+                        hpass_lean: bool = True, stream=None, out=None, evals=None):
         """Minimise in place on the device; returns (energy, status, iters) device tensors.
 
         ``evals`` (optional int32 device tensor, one per conformer) receives the
@@ -185,7 +187,7 @@ class Minimizer:
         else:
             e, st, it = out
         o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode, threads, ctas_per_sm,
-                       exit_test, check_every, atom_grad_scale, max_restarts, polish64)
+                       exit_test, check_every, atom_grad_scale, max_restarts, polish64, hpass_lean)
         bd, cd = self.batch.desc(), self.confs.desc()
         nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
         if nbytes == 0 and C > 0:
@@ -314,8 +316,8 @@ class BinnedMinimizer(Minimizer):
     def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
-                        atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None, stream=None,
-                        out=None, evals=None):
+                        atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
+                        hpass_lean: bool = True, stream=None, out=None, evals=None):
         torch = _torch()
         L = _lib.load()
         C = self.confs.n_conf
@@ -333,7 +335,8 @@ class BinnedMinimizer(Minimizer):
             cfg = b["cfg"]
             o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode,
                            threads or cfg.get("threads", 0), ctas_per_sm or cfg.get("ctas_per_sm", 0),
-                           exit_test, check_every, atom_grad_scale, max_restarts, polish64)
+                           exit_test, check_every, atom_grad_scale, max_restarts, polish64,
+                           bool(cfg.get("lean", hpass_lean)))
             cd = b["confs"].desc()
             nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
             if b["scratch"] is None or b["scratch"].numel() < nbytes:

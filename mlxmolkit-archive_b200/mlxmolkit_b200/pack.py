@@ -53,6 +53,10 @@ class PackedBatch:
     def max_atoms(self) -> int:
         return int(self.n_atoms.max()) if len(self.n_atoms) else 0
 
+    @property
+    def max_classes(self) -> int:
+        return int(self.mol_desc[:, MD_NCLS].max()) if len(self.mol_desc) else 1
+
     def nbytes(self) -> int:
         return sum(a.nbytes for a in (self.mol_desc, self.bonded, self.atom_cls, self.atom_q,
                                       self.cls_tab, self.pair_mask))
@@ -267,6 +271,8 @@ def pack_molecules(params_list) -> PackedBatch:
         if n > MAX_ATOMS:
             raise ValueError(f"molecule of {n} atoms exceeds {MAX_ATOMS}")
         tab, cls, q, mask, ncls = _nonbonded(p)
+        if ncls > 64:
+            raise ValueError(f"molecule with {ncls} non-bonded classes exceeds 64")
         recs = _bonded_records(p)
         d = np.zeros(MOL_DESC_INTS, dtype=np.int32)
         d[MD_N] = n

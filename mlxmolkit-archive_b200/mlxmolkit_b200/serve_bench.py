@@ -1,0 +1,72 @@
+"""Serving benchmark (config 4): Poisson arrivals, mixed sizes, p50/p99 latency.
+
+Each request is one seeded molecule (heavy atoms 10-80, MMFF94 / MMFF94s at
+random) with k ~ U{1..50} conformers.  Requests arrive as a Poisson stream at a
+given rate of conformers per second; ``MMFFServer`` admits them by device
+memory budget, runs them concurrently on CUDA streams and completes each one
+when its kernel ends.  For every swept rate the run reports the achieved
+throughput (converged conformers / s), p50 / p99 request latency, and whether
+the server kept up (queue drained within the run).  Molecules are drawn from
+a pre-generated pool so request generation does not throttle the arrivals.
+
+Usage: python -m mlxmolkit_b200.serve_bench --rates 500,2000,8000 --duration 20
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import synth
+from .serve import MMFFServer, poisson_stream
+
+
+def make_pool(n_mols: int, seed: int = 4):
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(1, 51, size=n_mols)
+    mols = synth.make_molecules(n_mols, [int(k) for k in ks], seed, 10, 80, max_atoms=170)
+    variants = ["MMFF94" if rng.random() < 0.5 else "MMFF94s" for _ in range(n_mols)]
+    return mols, variants
+
+
+def run_rate(pool, rate: float, duration: float, budget: int, seed: int = 0) -> dict:
+    mols, variants = pool
+    srv = MMFFServer(hbm_budget_bytes=budget)
+
+    def make_request(i):
+        j = i % len(mols)
+        m = mols[j]
+        xyz = np.stack([c.pos for c in m.GetConformers()])
+        return m, xyz, variants[j]
+
+    t0 = time.perf_counter()
+    futures = poisson_stream(srv, make_request, rate, duration, seed=seed)
+    results = [f.result() for f in futures]
+    t1 = time.perf_counter()
+    srv.close()
+    lat = np.array([r.latency for r in results])
+    confs = sum(len(r.energies) for r in results)
+    conv = sum(int(r.converged.sum()) for r in results)
+    wall = t1 - t0
+    return {"rate_confs_per_s": rate, "requests": len(results), "conformers": confs,
+            "converged": conv, "wall_s": wall, "converged_per_s": conv / wall,
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "kept_up": bool(wall <= duration * 1.2 + 5.0), "peak_mem_bytes": int(srv.peak_in_use)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rates", default="500,2000,8000")
+    ap.add_argument("--duration", type=float, default=20.0)
+    ap.add_argument("--pool", type=int, default=300)
+    ap.add_argument("--budget-gb", type=float, default=16.0)
+    a = ap.parse_args()
+    pool = make_pool(a.pool)
+    rows = [run_rate(pool, float(r), a.duration, int(a.budget_gb * (1 << 30))) for r in a.rates.split(",")]
+    print(json.dumps({"serving": rows}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -307,14 +307,15 @@ def _attach_sites(sk: _Skeleton, rng: np.random.Generator, exclude_halo=True):
 def generate_molecule(rng: np.random.Generator, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macrocycle: bool = False,
                       max_rotatable: int | None = None, name: str = "",
-                      max_tries: int = 50, max_atoms: int | None = None) -> SynthMol:
+                      max_tries: int = 50, max_atoms: int | None = None,
+                      ring_density: float = 0.0) -> SynthMol:
     """Grow one seeded drug-like molecule (explicit H) of heavy_lo..heavy_hi heavy atoms.
 
     Draws that exceed max_rotatable rotatable bonds or max_atoms atoms (with H)
     are rejected and redrawn.
     """
     for _ in range(max_tries):
-        mol = _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name)
+        mol = _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_density)
         if mol is None:
             continue
         if max_rotatable is not None and count_rotatable(mol) > max_rotatable:
@@ -325,9 +326,14 @@ def generate_molecule(rng: np.random.Generator, heavy_lo: int, heavy_hi: int,
     raise RuntimeError("molecule generation failed repeatedly")
 
 
-def _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name):
+def _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_density=0.0):
     target = int(rng.integers(heavy_lo, heavy_hi + 1))
-    n_rings = int(rng.integers(0, max_rings + 1))
+    if ring_density > 0:
+        # ring-rich large molecules: about one ring per 1/ring_density heavy atoms
+        lo_r = int(target * ring_density * 0.7)
+        n_rings = int(rng.integers(lo_r, max(lo_r, int(target * ring_density * 1.3)) + 1))
+    else:
+        n_rings = int(rng.integers(0, max_rings + 1))
     sk = _Skeleton()
     ring_plan = []
     for _ in range(n_rings):
@@ -1029,13 +1035,14 @@ class Workload:
 def make_one_molecule(seed: int, m: int, k: int, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macro_frac: float = 0.0,
                       max_rotatable: int | None = None, noise: float = 0.1,
-                      max_atoms: int | None = None) -> SynthMol:
+                      max_atoms: int | None = None, ring_density: float = 0.0) -> SynthMol:
     """Molecule m of the seeded stream: its own generator seeded by (seed, m)."""
     rng = np.random.default_rng([seed, m])
     macro = macro_frac > 0 and rng.random() < macro_frac
     mol = generate_molecule(rng, heavy_lo, heavy_hi, max_rings=max_rings,
                             macrocycle=macro, max_rotatable=max_rotatable,
-                            name=f"synth-{seed}-{m}", max_atoms=max_atoms)
+                            name=f"synth-{seed}-{m}", max_atoms=max_atoms, ring_density=ring_density,
+                            max_tries=200)
     for c in embed_conformers(mol, int(k), rng, noise=noise):
         mol.AddConformer(c)
     return mol
@@ -1048,7 +1055,7 @@ def _make_one_star(args):
 def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_hi: int,
                    max_rings: int = 3, macro_frac: float = 0.0,
                    max_rotatable: int | None = None, noise: float = 0.1,
-                   workers: int | None = None, max_atoms: int | None = None):
+                   workers: int | None = None, max_atoms: int | None = None, ring_density: float = 0.0):
     """n_mols seeded molecules, each with k (or k[i]) embedded noisy conformers.
 
     Each molecule has its own generator seeded by (seed, index), so the result
@@ -1057,8 +1064,8 @@ def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_h
     import os
     ks = [int(k[m]) if isinstance(k, (list, tuple, np.ndarray)) else int(k)
           for m in range(n_mols)]
-    jobs = [(seed, m, ks[m], heavy_lo, heavy_hi, max_rings, macro_frac, max_rotatable, noise, max_atoms)
-            for m in range(n_mols)]
+    jobs = [(seed, m, ks[m], heavy_lo, heavy_hi, max_rings, macro_frac, max_rotatable, noise, max_atoms,
+             ring_density) for m in range(n_mols)]
     if workers is None:
         workers = min(os.cpu_count() or 1, 16) if n_mols >= 64 else 1
     if workers <= 1:
@@ -1087,6 +1094,7 @@ def make_workload(config: int, seed: int = 0, scale: float = 1.0) -> Workload:
         var = ["MMFF94" if i % 2 == 0 else "MMFF94s" for i in range(len(mols))]
         return Workload("cfg1-2000x10-heavy8-70", mols, var, 1000, False)
     if config == 3:
-        mols = make_molecules(n(500), 8, seed, 60, 160, macro_frac=0.3, max_rotatable=20)
+        mols = make_molecules(n(500), 8, seed, 60, 160, macro_frac=0.3, max_rotatable=20, max_atoms=400,
+                              ring_density=0.12)
         return Workload("cfg3-500x8-heavy60-160", mols, ["MMFF94"] * len(mols), 3000, True)
     raise ValueError(f"unknown config {config}")
