@@ -163,6 +163,45 @@ int mmffb_plain_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, co
 int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
                    const float *sd, float *pos, double *energy, mmffb_stream_t stream);
 
+/* Size of the fixed per-device scratch array behind mmffb_minimize_noalloc. */
+#define MMFFB_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+
+/*
+ * mmffb_minimize with no scratch argument and no device allocation.  This
+ * entry point has no counterpart in the reference.
+ *
+ * It is for callers that cannot allocate device memory at call time:
+ * - a serving loop whose other streams must keep running, since cudaMalloc
+ *   and cudaFree can synchronise the device;
+ * - a host whose device memory is reserved up front by another framework's
+ *   pool, where a cudaMalloc would fail or take memory the pool expects.
+ *
+ * Scratch comes from a fixed array inside this library,
+ * MMFFB_NOALLOC_SCRATCH_BYTES (64 MiB) per device.  It holds the work
+ * counter, the error word and one inverse-Hessian slot per CTA.  A dense BFGS
+ * slot is 3N x 3N elements (N = max_atoms): 4 B each for mixed and fp32,
+ * 8 B for fp64.  The call itself allocates nothing.
+ *
+ * - Set-up: the first call on a device, with that device current, looks up
+ *   the array's device address and caches it.  Make that first call before
+ *   any stream capture.
+ * - Limit: if the persistent grid's slots do not all fit in the array, the
+ *   grid shrinks to the slots that fit.  Results are unchanged; batches of
+ *   large molecules run on fewer CTAs (about 80 for 150 atoms in mixed
+ *   precision).  If even one slot plus 256 B does not fit, the call returns
+ *   MMFFB_ESCRATCH.
+ * - Concurrency: each device has one array.  Calls whose kernels overlap on
+ *   the GPU race on it and give wrong results; this happens with calls on
+ *   different streams or from several host threads.  Issue such calls on one
+ *   stream, or use mmffb_minimize with one scratch buffer per stream.
+ *
+ * Otherwise the arguments, results and error codes are those of
+ * mmffb_minimize.
+ */
+int mmffb_minimize_noalloc(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                           float *pos, double *energy, int32_t *status, int32_t *iters,
+                           int32_t *ls_evals, mmffb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,7 @@ static int device_props(int *sms, int *smem_optin) {
     return 0;
 }
 
-static int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c) {
+int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c) {
     if (!b || !c) return fail(MMFFB_EINVAL, "null batch or conformer descriptor");
     if (c->n_conf < 0 || b->n_mols < 0) return fail(MMFFB_EINVAL, "negative count");
     if (c->n_conf > 0 && (!b->mol_desc || !b->bonded || !b->atom_cls || !b->atom_q || !b->cls_tab ||
@@ -48,13 +48,13 @@ static int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c) {
     return 0;
 }
 
-static TermMode to_mode(const double *mode) {
+TermMode to_mode(const double *mode) {
     TermMode md;
     md.cb = mode[0]; md.kang = mode[1]; md.ksbg = mode[2]; md.lin = mode[3] != 0.0;
     return md;
 }
 
-static KConst to_consts(const double *k) {
+KConst to_consts(const double *k) {
     KConst K;
     K.tolx = k[0]; K.functol = k[1]; K.movetol = k[2]; K.eps = k[3]; K.maxstep = k[4];
     K.maxls = (int)k[5]; K.gscale = k[6]; K.gcap = k[7];
@@ -63,7 +63,7 @@ static KConst to_consts(const double *k) {
 
 // Pick the kernel instance (CTA size, register-cached H columns, matrix in
 // shared or global memory) and the persistent grid for these conformers.
-static int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl) {
+int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl) {
     int sms = 0, optin = 0;
     int r = device_props(&sms, &optin);
     if (r) return r;

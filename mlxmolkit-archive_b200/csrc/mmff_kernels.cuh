@@ -1127,4 +1127,10 @@ int energy_grad_mixed(const Params &P, float *grad, cudaStream_t st);
 int energy_grad_fp64(const Params &P, float *grad, cudaStream_t st);
 int energy_grad_fp32(const Params &P, float *grad, cudaStream_t st);
 
+// argument checks and launch planning shared by the C ABI entry points (mmff_capi.cu)
+int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c);
+TermMode to_mode(const double *mode);
+KConst to_consts(const double *k);
+int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl);
+
 }  // namespace mmffb
