@@ -652,6 +652,91 @@ struct Opt {
         fence_proxy_async_global();   // this pass's row stores before the next pass's TMA reads
     }
 
+    // The streamed pass of the register-lean FP32 instance: float4 columns (the
+    // rows of H and the vectors are padded to a multiple of 4 with zeros) and two
+    // rows per step, so each vector load from shared memory serves two rows and a
+    // warp keeps two row copies of its TMA ring in use at once.
+    __device__ __forceinline__ void hpass_stream_v4(bool pending) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int ldr = hld(3 * P.nmax);
+        float *rw = (float *)ring + (size_t)warp * kStages * ldr;
+        uint64_t *bw = mbar + warp * kStages;
+        const int nrows = warp < n ? (n - warp + NW - 1) / NW : 0;
+        const uint32_t bytes = (uint32_t)(ldh * sizeof(float));
+        const int n4 = ldh >> 2;
+        const float4 *X4 = (const float4 *)pxi, *C4 = (const float4 *)pc;
+        const float4 *G4 = (const float4 *)g, *D4 = (const float4 *)dg;
+        float *H = (float *)mat;
+        if (lane == 0) {
+            for (int t = 0; t < nrows && t < kStages; ++t) {
+                mbar_expect_tx(&bw[t], bytes);
+                tma_load_row(rw + (size_t)t * ldr, H + (size_t)(warp + NW * t) * ldh, bytes, &bw[t]);
+            }
+        }
+        for (int t = 0; t < nrows; t += 2) {
+            const bool two = t + 1 < nrows;
+            const int s0 = t % kStages, s1 = (t + 1) % kStages;
+            uint32_t spins = 0;
+            while (!mbar_try_wait(&bw[s0], (phase >> s0) & 1u)) {
+                if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
+            }
+            phase ^= 1u << s0;
+            if (two) {
+                spins = 0;
+                while (!mbar_try_wait(&bw[s1], (phase >> s1) & 1u)) {
+                    if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
+                }
+                phase ^= 1u << s1;
+            }
+            const int i0 = warp + NW * t, i1 = i0 + NW;
+            const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
+            float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
+            const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
+            const float r1 = (pending && two) ? (float)pr[i1] : 0.f, x1 = (pending && two) ? (float)pxi[i1] : 0.f;
+            float a0 = 0.f, q0 = 0.f, a1 = 0.f, q1 = 0.f;
+            for (int c = lane; c < n4; c += 32) {
+                float4 h0 = A0[c];
+                float4 h1 = two ? A1[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (pending) {
+                    const float4 px = X4[c], pv = C4[c];
+                    h0.x = fmaf(x0, pv.x, fmaf(px.x, r0, h0.x));
+                    h0.y = fmaf(x0, pv.y, fmaf(px.y, r0, h0.y));
+                    h0.z = fmaf(x0, pv.z, fmaf(px.z, r0, h0.z));
+                    h0.w = fmaf(x0, pv.w, fmaf(px.w, r0, h0.w));
+                    W0[c] = h0;
+                    if (two) {
+                        h1.x = fmaf(x1, pv.x, fmaf(px.x, r1, h1.x));
+                        h1.y = fmaf(x1, pv.y, fmaf(px.y, r1, h1.y));
+                        h1.z = fmaf(x1, pv.z, fmaf(px.z, r1, h1.z));
+                        h1.w = fmaf(x1, pv.w, fmaf(px.w, r1, h1.w));
+                        W1[c] = h1;
+                    }
+                }
+                const float4 gg = G4[c], dd = D4[c];
+                a0 = fmaf(h0.w, gg.w, fmaf(h0.z, gg.z, fmaf(h0.y, gg.y, fmaf(h0.x, gg.x, a0))));
+                q0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, q0))));
+                a1 = fmaf(h1.w, gg.w, fmaf(h1.z, gg.z, fmaf(h1.y, gg.y, fmaf(h1.x, gg.x, a1))));
+                q1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, q1))));
+            }
+            a0 = wsum(a0); q0 = wsum(q0); a1 = wsum(a1); q1 = wsum(q1);
+            if (lane == 0) {
+                hp[i0] = a0; hq[i0] = q0;
+                if (two) { hp[i1] = a1; hq[i1] = q1; }
+                fence_proxy_async_smem();
+                if (t + kStages < nrows) {
+                    mbar_expect_tx(&bw[s0], bytes);
+                    tma_load_row(rw + (size_t)s0 * ldr, H + (size_t)(warp + NW * (t + kStages)) * ldh, bytes, &bw[s0]);
+                }
+                if (t + 1 + kStages < nrows) {
+                    mbar_expect_tx(&bw[s1], bytes);
+                    tma_load_row(rw + (size_t)s1 * ldr, H + (size_t)(warp + NW * (t + 1 + kStages)) * ldh, bytes,
+                                 &bw[s1]);
+                }
+            }
+        }
+        fence_proxy_async_global();
+    }
+
     // L-BFGS two-loop recursion (lbfgs_tg.metal:264-292): dir = -H g from the ring history
     __device__ __forceinline__ void two_loop(int hcount, int hidx) {
         const int hm = P.hist_m;
@@ -721,6 +806,8 @@ struct Opt {
         }
         stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
         ldh = MSM ? n : hld(n);
+        // zero vector pads: the float4 pass reads columns up to hld(n)
+        for (int k = n + tid; k < nv; k += NT) { g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0); }
         if (!LB) reset_matrix();
         __syncthreads();
 
@@ -927,7 +1014,8 @@ struct Opt {
                 }
                 if (!LB) {
                     __syncthreads();
-                    if (MSM) hpass(pending);
+                    if constexpr (!MSM && NC == 0 && sizeof(R) == 4) hpass_stream_v4(pending);
+                    else if (MSM) hpass(pending);
                     else hpass_stream(pending);
                     __syncthreads();
                     A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};

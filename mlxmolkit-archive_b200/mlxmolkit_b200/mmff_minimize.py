@@ -298,6 +298,7 @@ class BinnedMinimizer(Minimizer):
         n_atoms = np.array([int(p.n_atoms) for p in self.params_list], dtype=np.int64)
         nconf = n_atoms[self.conf_mol]
         self.bins = []
+        self._bin_events = []
         lo = 0
         for hi in bins:
             sel = np.nonzero((nconf > lo) & (nconf <= hi))[0]
@@ -307,7 +308,7 @@ class BinnedMinimizer(Minimizer):
                 dc.n_conf = len(order)          # the bin's queue: its own order array
                 dc.max_atoms = int(nconf[sel].max())
                 cfg = dict((tuning or {}).get(str(hi), (tuning or {}).get(hi, {})))
-                self.bins.append({"hi": hi, "confs": dc, "n": len(order), "cfg": cfg,
+                self.bins.append({"hi": hi, "confs": dc, "n": len(order), "cfg": cfg, "sel": sel,
                                   "stream": torch.cuda.Stream(device=self.batch.device), "scratch": None,
                                   "cost": float(np.sum((3.0 * nconf[sel]) ** 2))})
             lo = hi
@@ -317,7 +318,10 @@ class BinnedMinimizer(Minimizer):
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
-                        hpass_lean: bool = True, stream=None, out=None, evals=None):
+                        hpass_lean: bool = True, stream=None, out=None, evals=None, time_bins=False):
+        """As ``Minimizer.minimize_device``, one launch per size class.  With
+        ``time_bins`` each launch is bracketed by timing events on its own stream;
+        ``bin_times_ms()`` reads them after a synchronize."""
         torch = _torch()
         L = _lib.load()
         C = self.confs.n_conf
@@ -327,6 +331,7 @@ class BinnedMinimizer(Minimizer):
             it = torch.empty(C, dtype=torch.int32, device=self.batch.device)
         else:
             e, st, it = out
+        self._bin_events = []
         main = stream if stream is not None else torch.cuda.current_stream()
         fork = torch.cuda.Event()
         fork.record(main)
@@ -343,16 +348,26 @@ class BinnedMinimizer(Minimizer):
                 b["scratch"] = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.batch.device)
             s = b["stream"]
             s.wait_event(fork)
+            if time_bins:
+                t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                t0.record(s)
             rc = L.mmffb_minimize(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), pos_dev.data_ptr(),
                                   e.data_ptr(), st.data_ptr(), it.data_ptr(),
                                   evals.data_ptr() if evals is not None else None, b["scratch"].data_ptr(),
                                   b["scratch"].numel(), ctypes.c_void_p(s.cuda_stream))
             _lib.check(rc, "mmffb_minimize")
+            if time_bins:
+                t1.record(s)
+                self._bin_events.append((b, t0, t1))
         for b in self.bins:
             ev = torch.cuda.Event()
             ev.record(b["stream"])
             main.wait_event(ev)
         return e, st, it
+
+    def bin_times_ms(self):
+        """[(bin upper bound, conformer indices, kernel ms)] of the last ``time_bins`` call."""
+        return [(b["hi"], b["sel"], t0.elapsed_time(t1)) for b, t0, t1 in self._bin_events]
 
 
 def mmff_minimize_nk(

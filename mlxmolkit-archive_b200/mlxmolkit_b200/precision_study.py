@@ -1,4 +1,4 @@
-"""Precision study on the config-1 inputs (config 2).
+"""Precision study on the drug-like workload (2000 molecules x 10 conformers, heavy atoms 8-70).
 
 Runs the same inputs three ways on the GPU:
 
@@ -28,7 +28,7 @@ from .mmff_params import extract_mmff_params
 
 def run(scale: float = 0.1, max_iters: int = 1000, seed: int = 0) -> dict:
     import torch
-    wl = synth.make_workload(2, seed=seed, scale=scale)
+    wl = synth.make_workload("druglike", seed=seed, scale=scale)
     params = [extract_mmff_params(m, mmff_variant=v) for m, v in zip(wl.mols, wl.variants)]
     counts = [m.GetNumConformers() for m in wl.mols]
     pos = np.concatenate([np.stack([c.pos for c in m.GetConformers()]).reshape(-1)
@@ -54,7 +54,7 @@ def run(scale: float = 0.1, max_iters: int = 1000, seed: int = 0) -> dict:
             rms[c] = np.sqrt(np.mean(gc * gc))
         out[name] = dict(e=e.cpu().numpy(), st=st.cpu().numpy(), it=it.cpu().numpy(), rms=rms, s=dt)
     ref = out["fp64"]["e"]
-    summary = {"workload": f"config-1 inputs x scale {scale}", "conformers": int(len(ref)),
+    summary = {"workload": f"druglike-2000x10-heavy8-70 x scale {scale}", "conformers": int(len(ref)),
                "max_iters": max_iters}
     for name, r in out.items():
         d = np.abs(r["e"] - ref)

@@ -1,0 +1,53 @@
+"""Small profiling case of the optimizer kernels, sized for an ncu capture.
+
+One size-binned minimisation of ``--mols`` seeded drug-like molecules x ``--k``
+conformers (heavy atoms 8-70, at most 150 atoms), mixed precision, dense
+BFGS, at most 1000 iterations.  At the defaults (60 x 10) the global-slot
+size class holds about 300 conformers of 75-150 atoms, whose inverse-Hessian
+slots (one per CTA, 296 CTAs) take more than the 126 MB L2, so DRAM counters
+keep their meaning, while the device holds well under 1 GB.
+
+Usage: python -m mlxmolkit_b200.profile_case [--mols 60] [--k 10] [--repeat 1]
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+from . import mmff_minimize as mm
+from . import synth
+from .mmff_params import extract_mmff_params
+from .roofline import algorithmic_bytes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--mols", type=int, default=60)
+    ap.add_argument("--k", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args()
+    import torch
+    mols = synth.make_molecules(a.mols, a.k, a.seed, 8, 70, max_atoms=150)
+    params = [extract_mmff_params(m) for m in mols]
+    pos = np.concatenate([np.stack([c.pos for c in m.GetConformers()]).reshape(-1)
+                          for m in mols]).astype(np.float32)
+    m = mm.BinnedMinimizer(params, [a.k] * len(mols))
+    x0 = torch.from_numpy(pos).cuda()
+    evals = torch.zeros(m.confs.n_conf, dtype=torch.int32, device=x0.device)
+    for _ in range(a.repeat):
+        x = x0.clone()
+        e, st, it = m.minimize_device(x, max_iters=1000, time_bins=True, evals=evals)
+        torch.cuda.synchronize()
+        e, it, ev = e.cpu().numpy(), it.cpu().numpy(), evals.cpu().numpy()
+        if not np.isfinite(e).all():
+            raise SystemExit("non-finite energies")
+        bins = [{"max_atoms": hi, "conformers": len(sel), "ms": round(ms, 2),
+                 "algorithmic_bytes": algorithmic_bytes(params, m.conf_mol[sel], it[sel], ev[sel])}
+                for hi, sel, ms in m.bin_times_ms()]
+        print(f"ok: {len(e)} conformers, mean iterations {it.mean():.1f}, size classes {bins}", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,28 @@
+"""Algorithmic bytes of a dense-BFGS minimisation, the numerator of the HBM roofline."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def term_bytes(p) -> int:
+    """Bytes of one molecule's term records in the reference's packed sizes."""
+    return (16 * len(p.bond_idx1) + 24 * len(p.angle_idx1) + 32 * len(p.strbend_idx1)
+            + 20 * len(p.oop_idx1) + 28 * len(p.torsion_idx1) + 16 * len(p.vdw_idx1)
+            + 20 * len(p.ele_idx1))
+
+
+def algorithmic_bytes(params, conf_mol, iters, evals) -> float:
+    """Algorithmic HBM bytes of minimising the conformers ``conf_mol`` (molecule indices).
+
+    Per iteration: the inverse Hessian read and written once (4-byte elements,
+    8 n^2 for n = 3N coordinates), 40 n for the BFGS vectors, the term records
+    and 24 B per atom of coordinates and gradient; per energy-only line-search
+    evaluation: the term records and 12 B per atom.
+    """
+    conf_mol = np.asarray(conf_mol)
+    n_atoms = np.array([p.n_atoms for p in params], dtype=np.float64)[conf_mol]
+    tb = np.array([term_bytes(p) for p in params], dtype=np.float64)[conf_mol]
+    n = 3 * n_atoms
+    per_iter = 8 * n * n + 40 * n + tb + 24 * n_atoms
+    per_eval = tb + 12 * n_atoms
+    return float(np.sum(np.asarray(iters, np.float64) * per_iter + np.asarray(evals, np.float64) * per_eval))

@@ -1,4 +1,4 @@
-"""Serving benchmark (config 4): Poisson arrivals, mixed sizes, p50/p99 latency.
+"""Serving benchmark: Poisson arrivals, mixed sizes, p50/p99 latency.
 
 Each request is one seeded molecule (heavy atoms 10-80, MMFF94 / MMFF94s at
 random) with k ~ U{1..50} conformers.  Requests arrive as a Poisson stream at a

@@ -1082,19 +1082,29 @@ def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_h
         return [_make_one_star(j) for j in jobs]
 
 
-def make_workload(config: int, seed: int = 0, scale: float = 1.0) -> Workload:
-    """The five benchmark configurations (scale < 1 shrinks the molecule count)."""
+WORKLOADS = ("small", "druglike", "large")
+
+
+def make_workload(name: str, seed: int = 0, scale: float = 1.0) -> Workload:
+    """A named benchmark workload (scale < 1 shrinks the molecule count).
+
+    * ``small``:    50 molecules x 50 conformers, heavy atoms 10-30, MMFF94, at most 2000 iterations;
+    * ``druglike``: 2000 molecules x 10 conformers, heavy atoms 8-70 (at most 150 atoms),
+      MMFF94 / MMFF94s alternating, dense BFGS, at most 1000 iterations;
+    * ``large``:    500 molecules x 8 conformers, heavy atoms 60-160 (at most 400 atoms),
+      30 % macrocycles, at most 20 rotatable bonds, L-BFGS, at most 3000 iterations.
+    """
     def n(x):
         return max(1, int(round(x * scale)))
-    if config == 0:
+    if name == "small":
         mols = make_molecules(n(50), 50, seed, 10, 30)
-        return Workload("cfg0-50x50-heavy10-30", mols, ["MMFF94"] * len(mols), 2000, False)
-    if config in (1, 2):
+        return Workload("small-50x50-heavy10-30", mols, ["MMFF94"] * len(mols), 2000, False)
+    if name == "druglike":
         mols = make_molecules(n(2000), 10, seed, 8, 70, max_atoms=150)
         var = ["MMFF94" if i % 2 == 0 else "MMFF94s" for i in range(len(mols))]
-        return Workload("cfg1-2000x10-heavy8-70", mols, var, 1000, False)
-    if config == 3:
+        return Workload("druglike-2000x10-heavy8-70", mols, var, 1000, False)
+    if name == "large":
         mols = make_molecules(n(500), 8, seed, 60, 160, macro_frac=0.3, max_rotatable=20, max_atoms=400,
                               ring_density=0.12)
-        return Workload("cfg3-500x8-heavy60-160", mols, ["MMFF94"] * len(mols), 3000, True)
-    raise ValueError(f"unknown config {config}")
+        return Workload("large-500x8-heavy60-160", mols, ["MMFF94"] * len(mols), 3000, True)
+    raise ValueError(f"unknown workload {name!r}; one of {WORKLOADS}")
