@@ -41,7 +41,12 @@ for _p in (os.path.join(ROOT, "mlxmolkit-archive_b200"), ROOT):
 
 METRIC = "converged conformers/sec at >=98% within 0.1 kcal/mol of FP64 min"
 UNIT = "conformers/s"
-WORKLOAD = "druglike: 2000 mols x 10 confs, heavy 8-70 (20-150 atoms), MMFF94/94s 50/50, dense BFGS, max 1000 it"
+WORKLOADS = {
+    "druglike": "druglike: 2000 mols x 10 confs, heavy 8-70 (20-150 atoms), MMFF94/94s 50/50, dense BFGS, max 1000 it",
+    "small": "small: 50 mols x 50 confs, heavy 10-30, MMFF94, dense BFGS, max 2000 it",
+    "large": "large: 500 mols x 8 confs, heavy 60-160 (150-400 atoms), 30% with a 12-18 macrocycle, <= 20 "
+             "rotatable bonds, MMFF94, L-BFGS m=8, max 3000 it",
+}
 
 
 def _args():
@@ -53,13 +58,14 @@ def _args():
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the 2000 molecules")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="conformers in the CPU baseline sample")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", default="druglike", choices=sorted(WORKLOADS))
     return ap.parse_args()
 
 
-def _workload(seed: int, scale: float):
+def _workload(name: str, seed: int, scale: float):
     from mlxmolkit_b200 import synth
     from mlxmolkit_b200.mmff_params import extract_mmff_params
-    wl = synth.make_workload("druglike", seed=seed, scale=scale)
+    wl = synth.make_workload(name, seed=seed, scale=scale)
     params = [extract_mmff_params(m, mmff_variant=v) for m, v in zip(wl.mols, wl.variants)]
     pos = np.concatenate([np.stack([c.pos for c in m.GetConformers()]).reshape(-1)
                           for m in wl.mols]).astype(np.float32)
@@ -81,11 +87,11 @@ def _cpu_sample(params, counts, pos, n_sample: int, seed: int = 7):
     return pick, sp, cm, x
 
 
-def _run_cpu(params, conf_mol, x, max_iters: int):
+def _run_cpu(params, conf_mol, x, max_iters: int, history_m: int = 0):
     from oracle import oracle
     t = time.perf_counter()
     xo, e, st, it = oracle.minimize(params, None, x, max_iters=max_iters, conf_mol=conf_mol,
-                                    consts=oracle.TG_CONSTS, n_threads=0)
+                                    consts=oracle.TG_CONSTS, n_threads=0, history_m=history_m)
     return time.perf_counter() - t, e, st, oracle.max_threads()
 
 
@@ -142,12 +148,13 @@ class _Clocks:
 def _reference_arm(a, rank: int, world: int):
     if rank != 0:
         return
-    wl, params, counts, pos = _workload(0, a.scale)
+    wl, params, counts, pos = _workload(a.workload, 0, a.scale)
+    hist = 8 if wl.use_lbfgs else 0
     steps = []
     cores = None
     pick, sp, cm, x = _cpu_sample(params, counts, pos, a.cpu_sample // 2)
     for s in range(a.warmup + a.steps):
-        dt, e, st, cores = _run_cpu(sp, cm, x, wl.max_iters)
+        dt, e, st, cores = _run_cpu(sp, cm, x, wl.max_iters, hist)
         conv = int(np.isin(st, (0, 2, 3, 5)).sum())
         if s >= a.warmup:
             steps.append((dt, conv))
@@ -157,11 +164,12 @@ def _reference_arm(a, rank: int, world: int):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD + "; CPU sample of %d conformers" % len(cm),
+            "config": {"workload": WORKLOADS[a.workload] + "; CPU sample of %d conformers" % len(cm),
                        "sample_conformers": int(len(cm))},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{len(cm)} seeded conformers of the workload, FP64 dense BFGS "
-                                       f"(reference TG semantics), all host threads"},
+                             "sample": f"{len(cm)} seeded conformers of the workload, FP64 "
+                                       f"{'L-BFGS' if hist else 'dense BFGS'} (reference TG semantics), "
+                                       f"all host threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's own implementation is Metal/MLX (Apple only); its CPU restatement "
                     "(FP64 C oracle) runs here"}
@@ -189,7 +197,8 @@ def main():
     from mlxmolkit_b200.roofline import algorithmic_bytes
 
     t_prep = time.perf_counter()
-    wl, params, counts, pos = _workload(rank, a.scale)
+    wl, params, counts, pos = _workload(a.workload, rank, a.scale)
+    hist = mm.LBFGS_M if wl.use_lbfgs else 0
     m = mm.BinnedMinimizer(params, counts, tuning=mm.load_tuning())
     t_prep = time.perf_counter() - t_prep
     C = m.confs.n_conf
@@ -203,7 +212,8 @@ def main():
     # iteration cap -- the stand-in for RDKit's MMFFOptimizeMoleculeConfs(maxIters=cap)
     work.copy_(start)
     t64 = time.perf_counter()
-    e64, st64, _ = m.minimize_device(work, max_iters=wl.max_iters, precision="fp64", consts=mm.RDKIT_CONSTS)
+    e64, st64, _ = m.minimize_device(work, max_iters=wl.max_iters, precision="fp64", consts=mm.RDKIT_CONSTS,
+                                     history_m=hist)
     e64 = e64.cpu().numpy()
     t64 = time.perf_counter() - t64
 
@@ -216,7 +226,7 @@ def main():
         e = torch.cuda.Event(enable_timing=True)
         s.record()
         th = time.perf_counter()
-        out = m.minimize_device(work, max_iters=wl.max_iters, evals=evals, time_bins=True)
+        out = m.minimize_device(work, max_iters=wl.max_iters, evals=evals, time_bins=True, history_m=hist)
         host_ms.append((time.perf_counter() - th) * 1e3)
         e.record()
         torch.cuda.synchronize()
@@ -266,7 +276,7 @@ def main():
         e = torch.cuda.Event(enable_timing=True)
         s.record()
         work.copy_(host_in, non_blocking=True)
-        ee, ss, ii = m.minimize_device(work, max_iters=wl.max_iters)
+        ee, ss, ii = m.minimize_device(work, max_iters=wl.max_iters, history_m=hist)
         host_out.copy_(work, non_blocking=True)
         host_e.copy_(ee, non_blocking=True)
         host_st.copy_(ss, non_blocking=True)
@@ -290,7 +300,7 @@ def main():
     bins = []
     for (hi, sel, _), bms in zip(bt, bin_mean):
         bb = algorithmic_bytes(params, m.conf_mol[sel], it_mix[sel].astype(np.float64),
-                               ev[sel].astype(np.float64))
+                               ev[sel].astype(np.float64), history_m=hist)
         bins.append({"max_atoms": int(hi), "conformers": int(len(sel)), "ends_at_ms": float(bms),
                      "algorithmic_bytes": bb})
     top = bins[0]
@@ -313,7 +323,7 @@ def main():
         pass
 
     plain = None
-    if not a.no_plain and rank == 0:
+    if not a.no_plain and rank == 0 and not hist:
         # the plain reference-design path on the first 10% of the molecules (it is slow)
         nsub = max(1, len(params) // 10)
         mp_ = mm.Minimizer(params[:nsub], counts[:nsub])
@@ -336,11 +346,12 @@ def main():
     cpu = None
     if rank == 0:
         pick, sp, cm, x = _cpu_sample(params, counts, pos, a.cpu_sample)
-        dt, ec, stc, cores = _run_cpu(sp, cm, x, wl.max_iters)
+        dt, ec, stc, cores = _run_cpu(sp, cm, x, wl.max_iters, hist)
         cconv = int(np.sum(np.abs(ec - e64[pick]) <= 0.1))
         cpu = {"value": cconv / dt, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{len(cm)} seeded conformers of the same workload; FP64 C restatement of the "
-                         f"reference in-kernel BFGS; converged = within 0.1 kcal/mol of the FP64 GPU min",
+                         f"reference in-kernel {'L-BFGS' if hist else 'BFGS'}; converged = within 0.1 kcal/mol "
+                         f"of the FP64 GPU min",
                "seconds": dt, "converged_frac": cconv / len(cm)}
 
     if rank == 0:
@@ -349,7 +360,7 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 terms/update, f64 sums+tests",
             "data": "synthetic (seeded RDKit-free generator; RDKit absent)",
-            "config": {"workload": WORKLOAD if a.scale == 1.0 else WORKLOAD + f" x scale {a.scale}",
+            "config": {"workload": WORKLOADS[a.workload] + ("" if a.scale == 1.0 else f" x scale {a.scale}"),
                        "molecules": len(params), "conformers": C, "parallelism": f"dp{world} (replicas)",
                        "l2": "flushed (256 MB write) between timed steps"},
             "converged_frac": conv / C, "converged_frac_one_sided": conv_one_sided / C,
