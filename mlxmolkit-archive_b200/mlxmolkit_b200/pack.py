@@ -309,6 +309,45 @@ def pack_molecules(params_list) -> PackedBatch:
         n_atoms=np.asarray(natoms, dtype=np.int32))
 
 
+def merge_packed(batches) -> PackedBatch:
+    """One PackedBatch holding the molecules of several, in order.
+
+    The tables are concatenated and every molecule descriptor's offsets shifted
+    by the sizes of the tables before it, so a batch packed molecule by molecule
+    (e.g. as requests arrive) merges without repacking.
+    """
+    batches = list(batches)
+    if not batches:
+        return pack_molecules([])
+    descs, bonded, clss, qs, tabs, masks, natoms = [], [], [], [], [], [], []
+    rec_off = atom_off = tab_off = mask_off = 0
+    for b in batches:
+        d = b.mol_desc.copy()
+        d[:, MD_ATOM_OFF] += atom_off
+        d[:, MD_CLS_OFF] += tab_off
+        d[:, MD_MASK_OFF] += mask_off
+        for t in range(5):
+            d[:, MD_B_OFF + 2 * t] += rec_off
+        descs.append(d)
+        bonded.append(b.bonded)
+        clss.append(b.atom_cls)
+        qs.append(b.atom_q)
+        tabs.append(b.cls_tab)
+        masks.append(b.pair_mask)
+        natoms.append(b.n_atoms)
+        rec_off += len(b.bonded)
+        atom_off += len(b.atom_cls)
+        tab_off += len(b.cls_tab)
+        mask_off += len(b.pair_mask)
+    return PackedBatch(
+        mol_desc=np.ascontiguousarray(np.concatenate(descs), dtype=np.int32),
+        bonded=np.ascontiguousarray(np.concatenate(bonded), dtype=np.uint32),
+        atom_cls=np.concatenate(clss).astype(np.int32), atom_q=np.concatenate(qs).astype(np.float64),
+        cls_tab=np.ascontiguousarray(np.concatenate(tabs), dtype=np.float32),
+        pair_mask=np.ascontiguousarray(np.concatenate(masks), dtype=np.uint32),
+        n_atoms=np.concatenate(natoms).astype(np.int32))
+
+
 def conformer_index(n_atoms_per_mol, conf_counts):
     """conf_mol (int32), conf_coord (int64 float offsets, molecule-major order) and total floats."""
     n_atoms_per_mol = np.asarray(n_atoms_per_mol, dtype=np.int64)

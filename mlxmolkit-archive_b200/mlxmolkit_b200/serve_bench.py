@@ -53,7 +53,8 @@ def run_rate(pool, rate: float, duration: float, budget: int, seed: int = 0) -> 
     return {"rate_confs_per_s": rate, "requests": len(results), "conformers": confs,
             "converged": conv, "wall_s": wall, "converged_per_s": conv / wall,
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "kept_up": bool(wall <= duration * 1.2 + 5.0), "peak_mem_bytes": int(srv.peak_in_use)}
+            "kept_up": bool(wall <= duration * 1.2 + 5.0), "peak_mem_bytes": int(srv.peak_in_use),
+            "launches": int(srv.launches), "mean_latency_ms": float(lat.mean() * 1e3)}
 
 
 def main():

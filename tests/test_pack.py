@@ -133,6 +133,15 @@ def test_batch_offsets_are_consistent():
     assert len(pb.pair_mask) == masks.sum()
 
 
+def test_merging_per_molecule_packs_equals_packing_the_batch():
+    mols, params, counts, pos = small_workload(n_mols=5, k=2)
+    whole = pack.pack_molecules(params)
+    merged = pack.merge_packed([pack.pack_molecules([p]) for p in params])
+    for f in ("mol_desc", "bonded", "atom_cls", "atom_q", "cls_tab", "pair_mask", "n_atoms"):
+        assert np.array_equal(getattr(whole, f), getattr(merged, f)), f
+    assert merged.max_classes == whole.max_classes
+
+
 def test_hybridization_survives_pickling_and_worker_pools():
     """Molecules built in spawned workers must type exactly like serially built ones."""
     import pickle

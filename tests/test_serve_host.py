@@ -1,0 +1,32 @@
+"""Host logic of the serving loop: size classes fix the launch shape of every molecule."""
+from mlxmolkit_b200 import serve
+
+
+def test_size_classes_depend_only_on_the_molecule():
+    assert serve.size_class(20, 50).nmax == 24
+    assert serve.size_class(30, 10).nmax == 48
+    c = serve.size_class(60, 10)
+    assert (c.nmax, c.max_classes, c.history_m) == (74, 32, 0)
+    assert serve.size_class(60, 40).key == ("dense", 149, 64)      # too many classes for the 74-atom shape
+    assert serve.size_class(149, 10).key == ("dense", 149)
+    assert serve.size_class(150, 10).history_m == 8                 # L-BFGS from 150 atoms
+    assert serve.size_class(350, 10).nmax == 400
+    assert serve.size_class(500, 10).nmax == 500
+
+
+def test_launch_scratch_bound_grows_with_conformers_up_to_the_grid():
+    c = serve.size_class(100, 10)
+    a, b, d = (serve.launch_scratch_bytes(c, k) for k in (1, 100, 10000))
+    assert a < b < d and d == serve.launch_scratch_bytes(c, 296)
+
+
+def test_topology_key_separates_graphs_types_and_variants():
+    from mlxmolkit_b200 import synth
+    a, b = synth.make_molecules(2, 1, 41, 8, 20, workers=1)
+    ka = serve.topology_key(a, "MMFF94")
+    assert ka == serve.topology_key(a.copy(), "MMFF94")
+    assert ka != serve.topology_key(b, "MMFF94")
+    assert ka != serve.topology_key(a, "MMFF94s")
+    c = a.copy()
+    c.types[0] = "XX"
+    assert ka != serve.topology_key(c, "MMFF94")
