@@ -53,7 +53,9 @@ enum {
     MMFFB_ST_TOLX = 2,       /* step below TOLX */
     MMFFB_ST_SLOPE = 3,      /* no descent direction (slope >= 0) */
     MMFFB_ST_NONFINITE = 4,  /* energy or gradient not finite */
-    MMFFB_ST_LSFAIL = 5      /* line search found no decrease; position restored */
+    MMFFB_ST_LSFAIL = 5,     /* line search found no decrease; position restored */
+    MMFFB_ST_TIMEOUT = 6     /* a bounded wait on a data copy inside the kernel gave up: the
+                                result is not valid; the CTA stopped taking work (never expected) */
 };
 
 /* arithmetic of the optimizer */

@@ -191,6 +191,7 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 constexpr uint32_t kMaxWaitSpins = 1u << 22;   // bounded waits: give up, flag, never hang
+constexpr uint32_t kDrainSpins = 1u << 16;     // bounded wait for copies still in flight after giving up
 
 template <class R> __device__ __forceinline__ R qprod(double a, double b);
 template <> __device__ __forceinline__ float qprod<float>(double a, double b) { return (float)(a * b); }
@@ -448,6 +449,7 @@ struct Opt {
     R *ring;           // TMA row ring (streamed H pass)
     uint64_t *mbar;    // one mbarrier per ring stage and warp
     uint32_t phase;    // parity of each of this warp's stages
+    int *abort_flag;   // CTA-wide: a bounded wait gave up (shared memory)
     int ldh;           // row stride of H
     bool use64;        // line-search energies in FP64 (escalated)
     int *cls;
@@ -461,7 +463,7 @@ struct Opt {
     MolV m;
     int N, n, nv;
 
-    __device__ Opt(const Params &p, unsigned char *sm) : P(p), rsel(0) {
+    __device__ Opt(const Params &p, unsigned char *sm, int *abort_ = nullptr) : P(p), abort_flag(abort_), rsel(0) {
         Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes);
         pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
         pos4d = (double *)(sm + L.pos4d);
@@ -518,6 +520,36 @@ struct Opt {
         const int o = 4 * (k / 3) + (k % 3);
         pos4[o] = v;
         if (sizeof(R) == 4) pos4d[o] = (double)v;
+    }
+
+    // Warp-uniform bounded wait for ring stage st of this warp.  On giving up it
+    // flags the launch (err word) and this CTA (abort flag) and returns false.
+    __device__ __forceinline__ bool wait_stage(uint64_t *bw, int st) {
+        uint32_t spins = 0;
+        for (;;) {
+            const bool done = mbar_try_wait(&bw[st], (phase >> st) & 1u);
+            if (__all_sync(0xffffffffu, done)) break;
+            if (++spins > kMaxWaitSpins) {
+                if ((threadIdx.x & 31) == 0) {
+                    atomicExch(P.err, 1);
+                    atomicExch(abort_flag, 1);
+                }
+                return false;
+            }
+        }
+        phase ^= 1u << st;
+        return true;
+    }
+    // After a wait gave up: bounded wait for this warp's copies of rows [from, to) still
+    // in flight, so none lands in shared memory after the CTA has moved on or exited.
+    __device__ __forceinline__ void drain(uint64_t *bw, int from, int to) {
+        for (int t = from; t < to; ++t) {
+            const int st = t % kStages;
+            uint32_t spins = 0;
+            while (!__all_sync(0xffffffffu, mbar_try_wait(&bw[st], (phase >> st) & 1u)) && ++spins < kDrainSpins) {
+            }
+            phase ^= 1u << st;
+        }
     }
 
     // One pass over the dense inverse Hessian: apply the pending rank-2 update
@@ -601,11 +633,10 @@ struct Opt {
         }
         for (int t = 0; t < nrows; ++t) {
             const int st = t % kStages, i = warp + NW * t;
-            uint32_t spins = 0;
-            while (!mbar_try_wait(&bw[st], (phase >> st) & 1u)) {
-                if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
+            if (!wait_stage(bw, st)) {
+                drain(bw, t + 1, nrows < t + kStages ? nrows : t + kStages);
+                break;
             }
-            phase ^= 1u << st;
             const R *src = rw + (size_t)st * ldr;
             R *row = mat + (size_t)i * ldh;
             const R ri = pending ? pr[i] : R(0), xi = pending ? pxi[i] : R(0);
@@ -676,17 +707,14 @@ struct Opt {
         for (int t = 0; t < nrows; t += 2) {
             const bool two = t + 1 < nrows;
             const int s0 = t % kStages, s1 = (t + 1) % kStages;
-            uint32_t spins = 0;
-            while (!mbar_try_wait(&bw[s0], (phase >> s0) & 1u)) {
-                if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
+            const int issued = nrows < t + kStages ? nrows : t + kStages;
+            if (!wait_stage(bw, s0)) {
+                drain(bw, t + 1, issued);
+                break;
             }
-            phase ^= 1u << s0;
-            if (two) {
-                spins = 0;
-                while (!mbar_try_wait(&bw[s1], (phase >> s1) & 1u)) {
-                    if (++spins > kMaxWaitSpins) { if (lane == 0) atomicExch(P.err, 1); break; }
-                }
-                phase ^= 1u << s1;
+            if (two && !wait_stage(bw, s1)) {
+                drain(bw, t + 2, issued);
+                break;
             }
             const int i0 = warp + NW * t, i1 = i0 + NW;
             const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
@@ -1018,6 +1046,7 @@ struct Opt {
                     else if (MSM) hpass(pending);
                     else hpass_stream(pending);
                     __syncthreads();
+                    if (!MSM && *(volatile int *)abort_flag) { status = MMFFB_ST_TIMEOUT; break; }
                     A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};
                     for (int k = tid; k < n; k += NT) {
                         const R dgk = dg[k], xik = xo[k], qk = hq[k], gk = g[k];
@@ -1085,14 +1114,16 @@ template <class R, class A, int NT, int NC, bool MSM, bool LB>
 __global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_kernel(const Params P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
-    Opt<R, A, NT, NC, MSM, LB> opt(P, smem);
+    __shared__ int s_abort;
+    Opt<R, A, NT, NC, MSM, LB> opt(P, smem, &s_abort);
+    if (threadIdx.x == 0) s_abort = 0;
     if (!MSM && !LB) {
         if (threadIdx.x == 0) {
             for (int b = 0; b < (NT / 32) * kStages; ++b) mbar_init(&opt.mbar[b], 1);
             mbar_fence_init();
         }
-        __syncthreads();
     }
+    __syncthreads();
     const int *order = P.c.order;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
@@ -1101,6 +1132,7 @@ __global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_k
         __syncthreads();
         if (item >= P.c.n_conf) break;
         opt.run(order ? order[item] : item);
+        if (*(volatile int *)&s_abort) break;   // a copy never completed: stop taking work
     }
 }
 

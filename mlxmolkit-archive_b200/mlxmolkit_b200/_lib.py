@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libmmffb200.so")
 P = ctypes.c_void_p
 
 MMFFB_OK, MMFFB_EINVAL, MMFFB_ECUDA, MMFFB_ESCRATCH, MMFFB_ETOOBIG = 0, -1, -2, -3, -4
-ST_GRAD, ST_MAXIT, ST_TOLX, ST_SLOPE, ST_NONFINITE, ST_LSFAIL = 0, 1, 2, 3, 4, 5
+ST_GRAD, ST_MAXIT, ST_TOLX, ST_SLOPE, ST_NONFINITE, ST_LSFAIL, ST_TIMEOUT = 0, 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {0: "grad", 1: "max_iters", 2: "tolx", 3: "slope", 4: "nonfinite", 5: "line_search"}
 PREC = {"mixed": 0, "fp64": 1, "fp32": 2}
 EXIT_TG, EXIT_ATOM_NORM = 0, 1
