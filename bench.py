@@ -87,11 +87,14 @@ def _cpu_sample(params, counts, pos, n_sample: int, seed: int = 7):
     return pick, sp, cm, x
 
 
-def _run_cpu(params, conf_mol, x, max_iters: int, history_m: int = 0):
+def _run_cpu(params, conf_mol, x, max_iters: int, history_m: int = 0, rdkit_consts: bool = False):
+    """FP64 C oracle on all host threads: the reference in-kernel optimizer's constants, or
+    RDKit's (the stand-in for RDKit's MMFFOptimizeMoleculeConfs, the metric's FP64 minimum)."""
     from oracle import oracle
     t = time.perf_counter()
     xo, e, st, it = oracle.minimize(params, None, x, max_iters=max_iters, conf_mol=conf_mol,
-                                    consts=oracle.TG_CONSTS, n_threads=0, history_m=history_m)
+                                    consts=oracle.RDKIT_CONSTS if rdkit_consts else oracle.TG_CONSTS,
+                                    n_threads=0, history_m=history_m)
     return time.perf_counter() - t, e, st, oracle.max_threads()
 
 
@@ -346,12 +349,14 @@ def main():
     cpu = None
     if rank == 0:
         pick, sp, cm, x = _cpu_sample(params, counts, pos, a.cpu_sample)
-        dt, ec, stc, cores = _run_cpu(sp, cm, x, wl.max_iters, hist)
+        dt, ec, stc, cores = _run_cpu(sp, cm, x, wl.max_iters, hist, rdkit_consts=True)
         cconv = int(np.sum(np.abs(ec - e64[pick]) <= 0.1))
         cpu = {"value": cconv / dt, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{len(cm)} seeded conformers of the same workload; FP64 C restatement of the "
-                         f"reference in-kernel {'L-BFGS' if hist else 'BFGS'}; converged = within 0.1 kcal/mol "
-                         f"of the FP64 GPU min",
+               "sample": f"{len(cm)} seeded conformers of the same workload; FP64 C "
+                         f"{'L-BFGS' if hist else 'BFGS'} with RDKit's optimizer constants (the stand-in for "
+                         f"RDKit's MMFFOptimizeMoleculeConfs, absent here); converged = within 0.1 kcal/mol of "
+                         f"the FP64 GPU min, so converged_frac is the agreement of two FP64 runs that differ "
+                         f"only in rounding",
                "seconds": dt, "converged_frac": cconv / len(cm)}
 
     if rank == 0:

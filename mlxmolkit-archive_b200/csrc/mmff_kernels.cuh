@@ -274,7 +274,8 @@ template <> __device__ __forceinline__ double pair_charge<double>(const MolSmem 
 }
 
 // Copy a molecule's bit rows, class table, classes and charges into shared memory.
-template <int NT>
+// IR (the FP32 instances): stage 1/R* in place of R*, the pair term's only use of R*.
+template <int NT, bool IR = false>
 __device__ __forceinline__ void stage_molecule(const Params &P, const MolV &m, int *cls, double *qa, float *qf,
                                                uint32_t *mask, float2 *tab) {
     const int N = m.n, W = (N + 31) >> 5;
@@ -287,12 +288,17 @@ __device__ __forceinline__ void stage_molecule(const Params &P, const MolV &m, i
     const uint32_t *gm = P.b.pair_mask + m.mask_off;
     for (int k = threadIdx.x; k < 2 * N * W; k += NT) mask[k] = gm[k];
     const float2 *gt = reinterpret_cast<const float2 *>(P.b.cls_tab) + m.cls_off;
-    for (int k = threadIdx.x; k < m.ncls * m.ncls; k += NT) tab[k] = gt[k];
+    for (int k = threadIdx.x; k < m.ncls * m.ncls; k += NT) {
+        float2 v = gt[k];
+        if (IR) v.x = Num<float>::rcp(v.x > 1e-8f ? v.x : 1e-8f);
+        tab[k] = v;
+    }
 }
 
 // Energy (thread partial, not reduced) and -- if G -- per-warp gradient buffers.
-// pos4: smem float4-strided coordinates; gbuf: NW x nv.
-template <class R, class A, int NW, bool G>
+// pos4: smem float4-strided coordinates; gbuf: NW x nv.  IRTAB: the staged class
+// table holds 1/R* (see stage_molecule).
+template <class R, class A, int NW, bool G, bool IRTAB = false>
 __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R *pos4, R *gbuf,
                                         const MolSmem &ms, int nv) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -398,38 +404,68 @@ __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R 
     const int W = (N + 31) >> 5;
     const uint32_t *pm = ms.mask, *p14 = ms.mask + (size_t)N * W;
     const bool dd = m.diel == 2;
-    for (int i = warp; i < N - 1; i += NW) {
-        R xi, yi, zi;
+    // Rows i and i + NW per step: two independent pair chains per lane (both are
+    // evaluated; a pair absent from the bit rows contributes nothing) and one
+    // scatter per column.
+    for (int i = warp; i < N - 1; i += 2 * NW) {
+        const int i2 = i + NW;
+        const bool has2 = i2 < N - 1;
+        R xi, yi, zi, xk = R(0), yk = R(0), zk = R(0);
         ld3(pos4, i, xi, yi, zi);
-        const int ci = ms.cls[i] * m.ncls;
-        R fx = R(0), fy = R(0), fz = R(0);
+        if (has2) ld3(pos4, i2, xk, yk, zk);
+        const int ci = ms.cls[i] * m.ncls, ck = has2 ? ms.cls[i2] * m.ncls : 0;
+        const int ik = has2 ? i2 : i;
+        R fx = R(0), fy = R(0), fz = R(0), kx = R(0), ky = R(0), kz = R(0);
+        const int jb2 = has2 ? ((i2 + 1) & ~31) : N;
         for (int jb = (i + 1) & ~31; jb < N; jb += 32) {
-            const uint32_t wd = pm[i * W + (jb >> 5)];
-            if (wd == 0u) continue;
-            const uint32_t w14 = p14[i * W + (jb >> 5)];
-            if ((wd >> lane) & 1u) {
+            const int wb = jb >> 5;
+            const uint32_t wd = pm[i * W + wb];
+            const uint32_t wd2 = jb >= jb2 ? pm[i2 * W + wb] : 0u;
+            if ((wd | wd2) == 0u) continue;
+            const bool b1 = (wd >> lane) & 1u, b2 = (wd2 >> lane) & 1u;
+            if (b1 || b2) {
                 const int j = jb + lane;
-                const float2 t = ms.tab[ci + ms.cls[j]];
-                R qq = pair_charge<R>(ms, i, j);
-                if ((w14 >> lane) & 1u) qq *= R(0.75);
+                const int cj = ms.cls[j];
+                const float2 t1 = ms.tab[ci + cj], t2 = ms.tab[ck + cj];
+                const uint32_t w14 = p14[i * W + wb], w14b = jb >= jb2 ? p14[i2 * W + wb] : 0u;
+                R q1 = pair_charge<R>(ms, i, j), q2 = pair_charge<R>(ms, ik, j);
+                if ((w14 >> lane) & 1u) q1 *= R(0.75);
+                if ((w14b >> lane) & 1u) q2 *= R(0.75);
                 R xj, yj, zj;
                 ld3(pos4, j, xj, yj, zj);
-                const R dx = xi - xj, dy = yi - yj, dz = zi - zj;
-                R ev, ee, s;
-                pair_term<R, G>(dx, dy, dz, (R)t.x, (R)t.y, qq, dd, ev, ee, s);
-                acc += (A)ev;
-                acc += (A)ee;
+                const R dx1 = xi - xj, dy1 = yi - yj, dz1 = zi - zj;
+                const R dx2 = xk - xj, dy2 = yk - yj, dz2 = zk - zj;
+                R ev1, ee1, s1, ev2, ee2, s2;
+                pair_term<R, G, IRTAB>(dx1, dy1, dz1, (R)t1.x, (R)t1.y, q1, dd, ev1, ee1, s1);
+                pair_term<R, G, IRTAB>(dx2, dy2, dz2, (R)t2.x, (R)t2.y, q2, dd, ev2, ee2, s2);
+                if (b1) {
+                    acc += (A)ev1;
+                    acc += (A)ee1;
+                }
+                if (b2) {
+                    acc += (A)ev2;
+                    acc += (A)ee2;
+                }
                 if (G) {
-                    const R gx = s * dx, gy = s * dy, gz = s * dz;
-                    fx += gx; fy += gy; fz += gz;
-                    gw[3 * j] -= gx; gw[3 * j + 1] -= gy; gw[3 * j + 2] -= gz;
+                    const R m1 = b1 ? s1 : R(0), m2 = b2 ? s2 : R(0);
+                    const R g1x = m1 * dx1, g1y = m1 * dy1, g1z = m1 * dz1;
+                    const R g2x = m2 * dx2, g2y = m2 * dy2, g2z = m2 * dz2;
+                    fx += g1x; fy += g1y; fz += g1z;
+                    kx += g2x; ky += g2y; kz += g2z;
+                    gw[3 * j] -= g1x + g2x;
+                    gw[3 * j + 1] -= g1y + g2y;
+                    gw[3 * j + 2] -= g1z + g2z;
                 }
             }
         }
         if (G) {
             __syncwarp();
             fx = wsum(fx); fy = wsum(fy); fz = wsum(fz);
-            if (lane == 0) { gw[3 * i] += fx; gw[3 * i + 1] += fy; gw[3 * i + 2] += fz; }
+            kx = wsum(kx); ky = wsum(ky); kz = wsum(kz);
+            if (lane == 0) {
+                gw[3 * i] += fx; gw[3 * i + 1] += fy; gw[3 * i + 2] += fz;
+                if (has2) { gw[3 * i2] += kx; gw[3 * i2 + 1] += ky; gw[3 * i2 + 2] += kz; }
+            }
             __syncwarp();
         }
     }
@@ -496,9 +532,9 @@ struct Opt {
     __device__ __forceinline__ A energy() {
         A e[1];
         if (sizeof(R) == 4 && use64)
-            e[0] = (A)eval_terms<double, double, NW, false>(P, m, pos4d, (double *)nullptr, ms, nv);
+            e[0] = (A)eval_terms<double, double, NW, false, sizeof(R) == 4>(P, m, pos4d, (double *)nullptr, ms, nv);
         else
-            e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, ms, nv);
+            e[0] = eval_terms<R, A, NW, false, sizeof(R) == 4>(P, m, pos4, gbuf, ms, nv);
         A z[1] = {A(0)};
         reduce<1, 1>(e, z);
         return e[0];
@@ -506,7 +542,7 @@ struct Opt {
 
     // gradient at pos4 into dst (raw, unscaled); needs a preceding __syncthreads after pos4 writes
     __device__ __forceinline__ void gradient(R *dst) {
-        eval_terms<R, A, NW, true>(P, m, pos4, gbuf, ms, nv);
+        eval_terms<R, A, NW, true, sizeof(R) == 4>(P, m, pos4, gbuf, ms, nv);
         __syncthreads();
         for (int k = threadIdx.x; k < n; k += NT) {
             R s = R(0);
@@ -832,7 +868,7 @@ struct Opt {
             x[k] = v;
             setpos(k, v);
         }
-        stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
+        stage_molecule<NT, sizeof(R) == 4>(P, m, cls, qa, qf, mask, tab);
         ldh = MSM ? n : hld(n);
         // zero vector pads: the float4 pass reads columns up to hld(n)
         for (int k = n + tid; k < nv; k += NT) { g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0); }
@@ -1157,12 +1193,12 @@ __global__ void __launch_bounds__(NT) energy_grad_kernel(const Params P, float *
     const int n = 3 * m.n, nv = (3 * P.nmax + 3) & ~3;
     const float *gp = P.pos + P.c.conf_coord[conf];
     for (int k = threadIdx.x; k < n; k += NT) pos4[4 * (k / 3) + (k % 3)] = (R)gp[k];
-    stage_molecule<NT>(P, m, cls, qa, qf, mask, tab);
+    stage_molecule<NT, sizeof(R) == 4>(P, m, cls, qa, qf, mask, tab);
     const MolSmem ms{cls, qa, qf, mask, tab};
     __syncthreads();
     A e[1], z[1] = {A(0)};
-    if (grad) e[0] = eval_terms<R, A, NW, true>(P, m, pos4, gbuf, ms, nv);
-    else e[0] = eval_terms<R, A, NW, false>(P, m, pos4, gbuf, ms, nv);
+    if (grad) e[0] = eval_terms<R, A, NW, true, sizeof(R) == 4>(P, m, pos4, gbuf, ms, nv);
+    else e[0] = eval_terms<R, A, NW, false, sizeof(R) == 4>(P, m, pos4, gbuf, ms, nv);
     block_reduce<NW, 1, 1, A>(e, z, red);
     if (grad) {
         float *go = grad + P.c.conf_coord[conf];

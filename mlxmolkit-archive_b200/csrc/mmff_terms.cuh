@@ -243,13 +243,14 @@ __device__ __forceinline__ R torsion_term(const R* p1, const R* p2, const R* p3,
 // Returns the vdW and electrostatic energies separately (summed by the caller
 // in the same order as the reference's term loops) and the scalar radial
 // force factor s such that grad_i = s * (p_i - p_j), grad_j = -grad_i.
-template <class R, bool G>
+// IRIN: Rs already holds 1/R* (staged that way for the FP32 instances)
+template <class R, bool G, bool IRIN = false>
 __device__ __forceinline__ void pair_term(R dx, R dy, R dz, R Rs, R eps, R qq, bool dd,
                                           R& e_vdw, R& e_ele, R& s) {
     using N = Num<R>;
     R d2 = dx * dx + dy * dy + dz * dz;
     R d = N::sqrt_(maxR(d2, R(1e-16)));
-    R iR = N::rcp(maxR(Rs, R(1e-8)));
+    R iR = IRIN ? Rs : N::rcp(maxR(Rs, R(1e-8)));
     R q = d * iR;
     R q2 = q * q, q6 = q2 * q2 * q2, q7 = q6 * q;
     R ib = N::rcp(q + R(0.07));

