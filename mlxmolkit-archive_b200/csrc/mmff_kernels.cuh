@@ -558,6 +558,25 @@ struct Opt {
         if (sizeof(R) == 4) pos4d[o] = (double)v;
     }
 
+    // Butterfly reduce-scatter of 16 per-lane partial sums over the warp (16 shuffles):
+    // afterwards lanes l and l^1 both hold the warp-wide sum of value (l >> 1).
+    static __device__ __forceinline__ float reduce16(const float (&v)[16]) {
+        const int lane = threadIdx.x & 31;
+        const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+        float w[8], x[4], y[2];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            w[k] = (b4 ? v[k + 8] : v[k]) + __shfl_xor_sync(0xffffffffu, b4 ? v[k] : v[k + 8], 16);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            x[k] = (b3 ? w[k + 4] : w[k]) + __shfl_xor_sync(0xffffffffu, b3 ? w[k] : w[k + 4], 8);
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            y[k] = (b2 ? x[k + 2] : x[k]) + __shfl_xor_sync(0xffffffffu, b2 ? x[k] : x[k + 2], 4);
+        float z = (b1 ? y[1] : y[0]) + __shfl_xor_sync(0xffffffffu, b1 ? y[0] : y[1], 2);
+        return z + __shfl_xor_sync(0xffffffffu, z, 1);
+    }
+
     // Warp-uniform bounded wait for ring stage st of this warp.  On giving up it
     // flags the launch (err word) and this CTA (abort flag) and returns false.
     __device__ __forceinline__ bool wait_stage(uint64_t *bw, int st) {
@@ -740,62 +759,83 @@ struct Opt {
                 tma_load_row(rw + (size_t)t * ldr, H + (size_t)(warp + NW * t) * ldh, bytes, &bw[t]);
             }
         }
-        for (int t = 0; t < nrows; t += 2) {
-            const bool two = t + 1 < nrows;
-            const int s0 = t % kStages, s1 = (t + 1) % kStages;
-            const int issued = nrows < t + kStages ? nrows : t + kStages;
-            if (!wait_stage(bw, s0)) {
-                drain(bw, t + 1, issued);
-                break;
-            }
-            if (two && !wait_stage(bw, s1)) {
-                drain(bw, t + 2, issued);
-                break;
-            }
-            const int i0 = warp + NW * t, i1 = i0 + NW;
-            const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
-            float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
-            const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
-            const float r1 = (pending && two) ? (float)pr[i1] : 0.f, x1 = (pending && two) ? (float)pxi[i1] : 0.f;
-            float a0 = 0.f, q0 = 0.f, a1 = 0.f, q1 = 0.f;
-            for (int c = lane; c < n4; c += 32) {
-                float4 h0 = A0[c];
-                float4 h1 = two ? A1[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-                if (pending) {
-                    const float4 px = X4[c], pv = C4[c];
-                    h0.x = fmaf(x0, pv.x, fmaf(px.x, r0, h0.x));
-                    h0.y = fmaf(x0, pv.y, fmaf(px.y, r0, h0.y));
-                    h0.z = fmaf(x0, pv.z, fmaf(px.z, r0, h0.z));
-                    h0.w = fmaf(x0, pv.w, fmaf(px.w, r0, h0.w));
-                    W0[c] = h0;
-                    if (two) {
-                        h1.x = fmaf(x1, pv.x, fmaf(px.x, r1, h1.x));
-                        h1.y = fmaf(x1, pv.y, fmaf(px.y, r1, h1.y));
-                        h1.z = fmaf(x1, pv.z, fmaf(px.z, r1, h1.z));
-                        h1.w = fmaf(x1, pv.w, fmaf(px.w, r1, h1.w));
-                        W1[c] = h1;
+        // groups of 4 row pairs: the 16 per-lane partial sums are reduced together
+        for (int t0 = 0; t0 < nrows; t0 += 8) {
+            float v[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) v[k] = 0.f;
+            bool aborted = false;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int t = t0 + 2 * u;
+                if (t >= nrows) break;
+                const bool two = t + 1 < nrows;
+                const int s0 = t % kStages, s1 = (t + 1) % kStages;
+                const int issued = nrows < t + kStages ? nrows : t + kStages;
+                if (!wait_stage(bw, s0)) {
+                    drain(bw, t + 1, issued);
+                    aborted = true;
+                    break;
+                }
+                if (two && !wait_stage(bw, s1)) {
+                    drain(bw, t + 2, issued);
+                    aborted = true;
+                    break;
+                }
+                const int i0 = warp + NW * t, i1 = i0 + NW;
+                const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
+                float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
+                const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
+                const float r1 = (pending && two) ? (float)pr[i1] : 0.f, x1 = (pending && two) ? (float)pxi[i1] : 0.f;
+                float a0 = 0.f, q0 = 0.f, a1 = 0.f, q1 = 0.f;
+                for (int c = lane; c < n4; c += 32) {
+                    float4 h0 = A0[c];
+                    float4 h1 = two ? A1[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (pending) {
+                        const float4 px = X4[c], pv = C4[c];
+                        h0.x = fmaf(x0, pv.x, fmaf(px.x, r0, h0.x));
+                        h0.y = fmaf(x0, pv.y, fmaf(px.y, r0, h0.y));
+                        h0.z = fmaf(x0, pv.z, fmaf(px.z, r0, h0.z));
+                        h0.w = fmaf(x0, pv.w, fmaf(px.w, r0, h0.w));
+                        W0[c] = h0;
+                        if (two) {
+                            h1.x = fmaf(x1, pv.x, fmaf(px.x, r1, h1.x));
+                            h1.y = fmaf(x1, pv.y, fmaf(px.y, r1, h1.y));
+                            h1.z = fmaf(x1, pv.z, fmaf(px.z, r1, h1.z));
+                            h1.w = fmaf(x1, pv.w, fmaf(px.w, r1, h1.w));
+                            W1[c] = h1;
+                        }
+                    }
+                    const float4 gg = G4[c], dd = D4[c];
+                    a0 = fmaf(h0.w, gg.w, fmaf(h0.z, gg.z, fmaf(h0.y, gg.y, fmaf(h0.x, gg.x, a0))));
+                    q0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, q0))));
+                    a1 = fmaf(h1.w, gg.w, fmaf(h1.z, gg.z, fmaf(h1.y, gg.y, fmaf(h1.x, gg.x, a1))));
+                    q1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, q1))));
+                }
+                v[4 * u] = a0; v[4 * u + 1] = q0; v[4 * u + 2] = a1; v[4 * u + 3] = q1;
+                __syncwarp();   // every lane's reads of both stages before they are refilled
+                if (lane == 0) {
+                    fence_proxy_async_smem();
+                    if (t + kStages < nrows) {
+                        mbar_expect_tx(&bw[s0], bytes);
+                        tma_load_row(rw + (size_t)s0 * ldr, H + (size_t)(warp + NW * (t + kStages)) * ldh, bytes,
+                                     &bw[s0]);
+                    }
+                    if (t + 1 + kStages < nrows) {
+                        mbar_expect_tx(&bw[s1], bytes);
+                        tma_load_row(rw + (size_t)s1 * ldr, H + (size_t)(warp + NW * (t + 1 + kStages)) * ldh, bytes,
+                                     &bw[s1]);
                     }
                 }
-                const float4 gg = G4[c], dd = D4[c];
-                a0 = fmaf(h0.w, gg.w, fmaf(h0.z, gg.z, fmaf(h0.y, gg.y, fmaf(h0.x, gg.x, a0))));
-                q0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, q0))));
-                a1 = fmaf(h1.w, gg.w, fmaf(h1.z, gg.z, fmaf(h1.y, gg.y, fmaf(h1.x, gg.x, a1))));
-                q1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, q1))));
             }
-            a0 = wsum(a0); q0 = wsum(q0); a1 = wsum(a1); q1 = wsum(q1);
-            if (lane == 0) {
-                hp[i0] = a0; hq[i0] = q0;
-                if (two) { hp[i1] = a1; hq[i1] = q1; }
-                fence_proxy_async_smem();
-                if (t + kStages < nrows) {
-                    mbar_expect_tx(&bw[s0], bytes);
-                    tma_load_row(rw + (size_t)s0 * ldr, H + (size_t)(warp + NW * (t + kStages)) * ldh, bytes, &bw[s0]);
-                }
-                if (t + 1 + kStages < nrows) {
-                    mbar_expect_tx(&bw[s1], bytes);
-                    tma_load_row(rw + (size_t)s1 * ldr, H + (size_t)(warp + NW * (t + 1 + kStages)) * ldh, bytes,
-                                 &bw[s1]);
-                }
+            if (aborted) break;
+            // lanes l and l^1 now hold the sum of value l >> 1: pair u = value / 4, then a0 q0 a1 q1
+            const float sum = reduce16(v);
+            const int val = lane >> 1, tr = t0 + 2 * (val >> 2) + ((val >> 1) & 1);
+            if (!(lane & 1) && tr < nrows) {
+                const int i = warp + NW * tr;
+                if (val & 1) hq[i] = sum;
+                else hp[i] = sum;
             }
         }
         fence_proxy_async_global();
