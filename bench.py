@@ -197,10 +197,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     from mlxmolkit_b200 import mmff_minimize as mm
+    from mlxmolkit_b200.replicas import rank_seed, reduce_step
     from mlxmolkit_b200.roofline import algorithmic_bytes
 
     t_prep = time.perf_counter()
-    wl, params, counts, pos = _workload(a.workload, rank, a.scale)
+    wl, params, counts, pos = _workload(a.workload, rank_seed(0, rank), a.scale)
     hist = mm.LBFGS_M if wl.use_lbfgs else 0
     m = mm.BinnedMinimizer(params, counts, tuning=mm.load_tuning())
     t_prep = time.perf_counter() - t_prep
@@ -255,16 +256,7 @@ def main():
     dE = np.abs(e_mix - e64)
     conv = int(np.sum(dE <= 0.1))
     conv_one_sided = int(np.sum(e_mix - e64 <= 0.1))
-    ms_step = float(np.mean(times))
-    if dist:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
-        c = torch.tensor([conv], device=dev, dtype=torch.float64)
-        dist.all_reduce(c)
-        conv_all = float(c.item())
-    else:
-        conv_all = float(conv)
+    ms_step, conv_all = reduce_step(dist, float(np.mean(times)), conv, dev)
     value = conv_all / (ms_step / 1e3)
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
@@ -288,12 +280,8 @@ def main():
         if r >= a.warmup:
             e2e_ms.append(s.elapsed_time(e))
     e2e_conv = int(np.sum(np.abs(host_e.numpy() - e64) <= 0.1))
-    e2e_ms = float(np.mean(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = (e2e_conv * world) / (e2e_ms / 1e3)
+    e2e_ms, e2e_conv_all = reduce_step(dist, float(np.mean(e2e_ms)), e2e_conv, dev)
+    e2e_val = e2e_conv_all / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel: the size class with the most algorithmic bytes.
     # BinnedMinimizer launches it first, at the fork of the step, so the CUDA events on
