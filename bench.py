@@ -284,9 +284,10 @@ def main():
     e2e_val = e2e_conv_all / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel: the size class with the most algorithmic bytes.
-    # BinnedMinimizer launches it first, at the fork of the step, so the CUDA events on
-    # its own stream bracket exactly its kernel; the later classes' intervals also hold
-    # the time their CTAs waited for SMs, so they are reported as end times only.
+    # BinnedMinimizer launches the class of the largest molecules first, at the fork of the
+    # step, so the CUDA events on its own stream bracket exactly its kernel (on the drug-like
+    # workload that class is also the dominant one); a later class's interval also holds the
+    # time its CTAs waited for SMs, so it is reported as an end time.
     bin_mean = np.mean(np.array(bin_ms), axis=0)
     bins = []
     for (hi, sel, _), bms in zip(bt, bin_mean):
@@ -294,8 +295,8 @@ def main():
                                ev[sel].astype(np.float64), history_m=hist)
         bins.append({"max_atoms": int(hi), "conformers": int(len(sel)), "ends_at_ms": float(bms),
                      "algorithmic_bytes": bb})
-    top = bins[0]
-    assert top["algorithmic_bytes"] == max(b["algorithmic_bytes"] for b in bins)
+    top = max(bins, key=lambda b: b["algorithmic_bytes"])
+    top_first = top is bins[0]   # launched first: its interval is its own kernel time
     abytes = top["algorithmic_bytes"]
     achieved = abytes / (top["ends_at_ms"] / 1e3) / 1e9
     peaks = {}
@@ -369,6 +370,7 @@ def main():
                          "kernel": f"minimize_kernel, size class <= {top['max_atoms']} atoms "
                                    f"({top['conformers']} conformers, {top['ends_at_ms']:.1f} ms/launch)",
                          "algorithmic_bytes_per_launch": abytes, "size_classes": bins,
+                         "duration": "own kernel" if top_first else "upper bound (includes waiting for SMs)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback",
                          "note": "algorithmic bytes = 8n^2 + 40n + term bytes + 24N per iteration, term bytes "
                                  "+ 12N per line-search evaluation (n = 3N); traffic scaled from an ncu capture "

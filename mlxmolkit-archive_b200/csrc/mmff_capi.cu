@@ -76,7 +76,9 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     if (o->history_m < 0 || o->history_m > kMaxHist) return fail(MMFFB_EINVAL, "history_m out of range");
     const bool lb = o->history_m > 0;
     int nt = o->threads;
-    if (nt == 0) nt = nmax <= 24 ? 64 : (nmax <= 48 ? 128 : 256);
+    // default CTA size: 128 threads for 25-48 atoms, 256 otherwise (measured per size class on
+    // B200; for up to 24 atoms 256 threads beat 64 by finishing each conformer sooner)
+    if (nt == 0) nt = (nmax > 24 && nmax <= 48) ? 128 : 256;
     if (nt != 64 && nt != 128 && nt != 256 && nt != 512)
         return fail(MMFFB_EINVAL, "threads must be 64, 128, 256 or 512");
     if (!mixed || lb) nt = 256;
@@ -85,6 +87,9 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     if (nt == 512 && (lb || !mixed)) nt = 256;
     Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as, mc);
     bool msm = Ls.total <= (size_t)optin;
+    // mixed-precision dense BFGS above 48 atoms: the register-lean streamed instance (H in a
+    // global slot, 2 CTAs/SM) beats a shared-memory H that leaves one CTA of 8 warps per SM
+    if (mixed && !lb && nmax > 48) msm = false;
     int nc = 2;
     if (!lb) {
         if (msm) {

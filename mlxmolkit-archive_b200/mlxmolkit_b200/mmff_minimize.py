@@ -278,7 +278,10 @@ class Minimizer:
         return pos_dev.cpu().numpy(), e.cpu().numpy()
 
 
-DEFAULT_BINS = (24, 42, 74, 170, 1024)   # atom-count upper bounds of the size classes
+# atom-count upper bounds of the size classes: each class maps to one kernel instance of the
+# default plan (256 threads / shared-memory H; 128 threads / shared-memory H; register-lean
+# global-slot H; L-BFGS or larger), so no two classes run the same instance
+DEFAULT_BINS = (24, 48, 170, 1024)
 
 
 class BinnedMinimizer(Minimizer):
@@ -312,7 +315,9 @@ class BinnedMinimizer(Minimizer):
                                   "stream": torch.cuda.Stream(device=self.batch.device), "scratch": None,
                                   "cost": float(np.sum((3.0 * nconf[sel]) ** 2))})
             lo = hi
-        self.bins.sort(key=lambda b: -b["cost"])
+        # largest molecules first: their conformers take longest, and a class launched
+        # earlier takes the SMs first (longest-processing-time order across classes)
+        self.bins.sort(key=lambda b: -b["hi"])
 
     def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
