@@ -28,8 +28,7 @@ is bit-for-bit the same alone or in any mix of requests.
 |---------|-------------|------------|-------------------|
 | <= 24   | dense BFGS  | 24         | 64                |
 | 25-48   | dense BFGS  | 48         | 64                |
-| 49-74   | dense BFGS  | 74         | 32                |
-| 75-149  | dense BFGS  | 149        | 32                |
+| 49-149  | dense BFGS  | 149        | 32                |
 | 49-149 with more than 32 non-bonded classes | dense BFGS | 149 | 64 |
 | 150-300 | L-BFGS m=8  | 300        | 64                |
 | 301-400 | L-BFGS m=8  | 400        | 64                |
@@ -95,8 +94,6 @@ def size_class(n_atoms: int, n_classes: int) -> SizeClass:
         return SizeClass(("dense", 48), 48, 64, 0)
     if n_classes > 32:
         return SizeClass(("dense", 149, 64), 149, 64, 0)
-    if n_atoms <= 74:
-        return SizeClass(("dense", 74), 74, 32, 0)
     return SizeClass(("dense", 149), 149, 32, 0)
 
 

@@ -6,8 +6,8 @@ def test_size_classes_depend_only_on_the_molecule():
     assert serve.size_class(20, 50).nmax == 24
     assert serve.size_class(30, 10).nmax == 48
     c = serve.size_class(60, 10)
-    assert (c.nmax, c.max_classes, c.history_m) == (74, 32, 0)
-    assert serve.size_class(60, 40).key == ("dense", 149, 64)      # too many classes for the 74-atom shape
+    assert (c.nmax, c.max_classes, c.history_m) == (149, 32, 0)
+    assert serve.size_class(60, 40).key == ("dense", 149, 64)      # too many classes for the 32-class shape
     assert serve.size_class(149, 10).key == ("dense", 149)
     assert serve.size_class(150, 10).history_m == 8                 # L-BFGS from 150 atoms
     assert serve.size_class(350, 10).nmax == 400
