@@ -165,6 +165,19 @@ int mmffb_plain_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, co
 int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
                    const float *sd, float *pos, double *energy, mmffb_stream_t stream);
 
+/*
+ * Host-side packing helper (no device work): chunk ids of a term type's terms,
+ * the bonded-table layout above.  Greedy first fit in term order, at most 32
+ * terms per chunk and no atom twice in one role of a chunk; with flip_perm
+ * (the role permutation of the term's equivalent reversed form, or NULL) a term
+ * may enter a chunk reversed, flagged in flipped_out (may be NULL).
+ * role_atoms: int32[n_terms * roles], atoms < n_atoms.  Returns the number of
+ * chunks or a negative MMFFB_E* code.  Replaces the host packing loops of
+ * mlxmolkit/mmff_minimize.py:40-173 and mmff_metal_kernel.py:512-687.
+ */
+int32_t mmffb_pack_chunk(int32_t n_terms, int32_t roles, const int32_t *role_atoms, const int32_t *flip_perm,
+                         int32_t n_atoms, int64_t *chunk_out, uint8_t *flipped_out);
+
 /* Size of the fixed per-device scratch array behind mmffb_minimize_noalloc. */
 #define MMFFB_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 

@@ -44,7 +44,7 @@ class MMFFOptParams(ctypes.Structure):
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc"]
+           "mmffb_minimize_noalloc", "mmffb_pack_chunk"]
 
 _lib = None
 
@@ -77,6 +77,8 @@ def load():
     L.mmffb_plain_minimize.argtypes = [BP, CP, OP, P, P, P, P, P, ctypes.c_size_t, P]
     L.mmffb_fused_sd.restype = ctypes.c_int
     L.mmffb_fused_sd.argtypes = [BP, CP, OP, P, P, P, P]
+    L.mmffb_pack_chunk.restype = ctypes.c_int32
+    L.mmffb_pack_chunk.argtypes = [ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_int32, P, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int
     L.mmffb_minimize_noalloc.argtypes = [BP, CP, OP, P, P, P, P, P, P]
     _lib = L

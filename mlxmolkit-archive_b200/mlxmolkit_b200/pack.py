@@ -63,7 +63,26 @@ class PackedBatch:
 
 
 def _chunk(role_atoms: np.ndarray, flip_perm=None):
-    """Chunk id (and orientation) of every term.
+    """Chunk id (and orientation) of every term: the native chunker of libmmffb200.so.
+
+    Same rule and result as ``chunk_reference`` below, which the tests compare it with.
+    """
+    from . import _lib
+    ra = np.ascontiguousarray(role_atoms, dtype=np.int32)
+    T, R = ra.shape
+    out = np.empty(T, dtype=np.int64)
+    flipped = np.zeros(T, dtype=np.uint8)
+    fp = None if flip_perm is None else np.ascontiguousarray(flip_perm, dtype=np.int32)
+    n_atoms = int(ra.max()) + 1 if T else 1
+    rc = _lib.load().mmffb_pack_chunk(T, R, ra.ctypes.data, None if fp is None else fp.ctypes.data, n_atoms,
+                                      out.ctypes.data, flipped.ctypes.data)
+    if rc < 0:
+        raise ValueError(f"mmffb_pack_chunk failed ({rc})")
+    return out, flipped.astype(bool)
+
+
+def chunk_reference(role_atoms: np.ndarray, flip_perm=None):
+    """Chunk id (and orientation) of every term (the rule in Python).
 
     At most 32 terms per chunk and, per role, no atom twice in a chunk.
     role_atoms: (T, R) int.  flip_perm: the role permutation of the term's

@@ -154,3 +154,19 @@ def test_hybridization_survives_pickling_and_worker_pools():
         assert np.array_equal(pa.torsion_idx1, pb.torsion_idx1)
         assert np.array_equal(pa.strbend_idx2, pb.strbend_idx2)
         assert np.array_equal(x.GetConformer(0).pos, y.GetConformer(0).pos)
+
+
+def test_native_chunker_equals_the_python_rule():
+    mols, params, counts, pos = small_workload(n_mols=8, k=1, seed=17, lo=20, hi=60)
+    rng = np.random.default_rng(5)
+    cases = []
+    for p in params:
+        cases.append((np.stack([p.torsion_idx1, p.torsion_idx2, p.torsion_idx3, p.torsion_idx4], 1), (3, 2, 1, 0)))
+        cases.append((np.stack([p.angle_idx1, p.angle_idx2, p.angle_idx3], 1), (2, 1, 0)))
+        cases.append((np.stack([p.bond_idx1, p.bond_idx2], 1), None))
+    cases.append((rng.integers(0, 40, size=(500, 3)), (2, 1, 0)))      # many collisions
+    cases.append((np.zeros((0, 2), dtype=np.int64), (1, 0)))
+    for ra, fp in cases:
+        a, fa = pack._chunk(ra, fp)
+        b, fb = pack.chunk_reference(ra, fp)
+        assert np.array_equal(a, b) and np.array_equal(fa, fb)
