@@ -166,7 +166,8 @@ int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
                    const float *sd, float *pos, double *energy, mmffb_stream_t stream);
 
 /*
- * Host-side packing helper (no device work): chunk ids of a term type's terms,
+ * Host-side packing helper (no device work; unlike the calls above, every pointer
+ * here is host memory): chunk ids of a term type's terms,
  * the bonded-table layout above.  Greedy first fit in term order, at most 32
  * terms per chunk and no atom twice in one role of a chunk; with flip_perm
  * (the role permutation of the term's equivalent reversed form, or NULL) a term
