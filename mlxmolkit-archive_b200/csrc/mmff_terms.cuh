@@ -249,7 +249,15 @@ __device__ __forceinline__ void pair_term(R dx, R dy, R dz, R Rs, R eps, R qq, b
                                           R& e_vdw, R& e_ele, R& s) {
     using N = Num<R>;
     R d2 = dx * dx + dy * dy + dz * dz;
-    R d = N::sqrt_(maxR(d2, R(1e-16)));
+    const R x2 = maxR(d2, R(1e-16));
+    R d, rd;                                   // distance and (FP32) its reciprocal
+    if constexpr (sizeof(R) == 4) {
+        rd = N::rsqrt_(x2);                    // one reciprocal square root gives both
+        d = x2 * rd;
+    } else {
+        d = N::sqrt_(x2);
+        rd = R(0);
+    }
     R iR = IRIN ? Rs : N::rcp(maxR(Rs, R(1e-8)));
     R q = d * iR;
     R q2 = q * q, q6 = q2 * q2 * q2, q7 = q6 * q;
@@ -263,7 +271,9 @@ __device__ __forceinline__ void pair_term(R dx, R dy, R dz, R Rs, R eps, R qq, b
     R cq = R(MMFF_ELEC) * qq;
     e_ele = dd ? cq * idp * idp : cq * idp;
     if (G) {
-        R inv = d > R(1e-8) ? N::rcp(d) : R(0);
+        R inv;
+        if constexpr (sizeof(R) == 4) inv = d > R(1e-8) ? rd : R(0);
+        else inv = d > R(1e-8) ? N::rcp(d) : R(0);
         R dv = eps * iR * t7 * (R(-7.84) * q6 * iq * iq + (R(-7.84) * iq + R(14)) * ib);
         R de = dd ? R(-2) * cq * idp * idp * idp : -cq * idp * idp;
         s = (dv + de) * inv;
