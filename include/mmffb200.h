@@ -179,6 +179,54 @@ int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
 int32_t mmffb_pack_chunk(int32_t n_terms, int32_t roles, const int32_t *role_atoms, const int32_t *flip_perm,
                          int32_t n_atoms, int64_t *chunk_out, uint8_t *flipped_out);
 
+/*
+ * The reference's multi-molecule L-BFGS optimizer (mlxmolkit/mmff_metal_optimizer.py:217-535,
+ * behind mmff_optimize_metal_multi_mol), run as device-resident chunks: each
+ * mmffb_multimol_step launch advances every conformer by n_iters iterations of
+ * two-loop L-BFGS on the grad_scale-scaled gradient, a per-atom step cap of
+ * max_step_per_atom and no line search; energies use the given term mode (the
+ * reference uses its mega-kernel constants).  All state lives in the caller's
+ * device buffers below, laid out like the positions where noted.
+ */
+typedef struct {
+    float *x;               /* positions (like pos) */
+    float *g;               /* grad_scale * dE/dx at x (like pos) */
+    float *best_x;          /* best-seen positions (like pos) */
+    double *e;              /* energy at x, per conformer */
+    double *best_e;         /* best-seen energy, per conformer */
+    float *hist;            /* per conformer mmffb_multimol_hist_floats(): S rows, then Y rows */
+    float *rho;             /* per conformer history_m curvature factors */
+    int32_t *hcount;        /* pairs pushed so far, per conformer */
+    int32_t *converged;     /* main loop: met grad_tol at a check point (sticky) */
+    int32_t *conv_iter;     /* iteration of that check point (max_iters if never) */
+    int32_t *pending;       /* one counter: conformers that fail the test of the launch's check;
+                               the caller zeroes it before a checking launch */
+} MMFFMultiMolState;
+
+typedef struct {
+    int32_t history_m;      /* L-BFGS pairs, 1..16 (the reference's lbfgs_m) */
+    float grad_scale;
+    float max_step_per_atom;
+    float grad_tol;         /* largest per-atom norm of the scaled gradient */
+    double mode[4];         /* term constants, as MMFFOptParams.mode */
+} MMFFMultiMolParams;
+
+enum {
+    MMFFB_MM_START = 0,        /* E, g at x; best = x; history, converged and conv_iter reset */
+    MMFFB_MM_REVERT = 1,       /* x = best_x; E, g at x; history reset (the polish pass start) */
+    MMFFB_MM_RUN = 2,          /* n_iters iterations, no check */
+    MMFFB_MM_MAIN_CHECK = 3,   /* n_iters iterations, then best-seen update and the sticky test
+                                  (conv_iter = it_end); pending += conformers not converged */
+    MMFFB_MM_POLISH_CHECK = 4  /* n_iters iterations, then best-seen update; pending +=
+                                  conformers over grad_tol now */
+};
+
+/* Floats of history per conformer (2 * history_m rows of the padded coordinate count). */
+size_t mmffb_multimol_hist_floats(const MMFFConfDev *confs, int32_t history_m);
+int mmffb_multimol_step(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFMultiMolParams *params,
+                        const MMFFMultiMolState *state, int32_t phase, int32_t n_iters, int32_t it_end,
+                        int32_t max_iters, mmffb_stream_t stream);
+
 /* Size of the fixed per-device scratch array behind mmffb_minimize_noalloc. */
 #define MMFFB_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 

@@ -42,9 +42,22 @@ class MMFFOptParams(ctypes.Structure):
                 ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32)]
 
 
+class MMFFMultiMolState(ctypes.Structure):
+    _fields_ = [(f, P) for f in ("x", "g", "best_x", "e", "best_e", "hist", "rho", "hcount", "converged",
+                                 "conv_iter", "pending")]
+
+
+class MMFFMultiMolParams(ctypes.Structure):
+    _fields_ = [("history_m", ctypes.c_int32), ("grad_scale", ctypes.c_float),
+                ("max_step_per_atom", ctypes.c_float), ("grad_tol", ctypes.c_float),
+                ("mode", ctypes.c_double * 4)]
+
+
+MM_START, MM_REVERT, MM_RUN, MM_MAIN_CHECK, MM_POLISH_CHECK = 0, 1, 2, 3, 4
+
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc", "mmffb_pack_chunk"]
+           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step"]
 
 _lib = None
 
@@ -77,6 +90,11 @@ def load():
     L.mmffb_plain_minimize.argtypes = [BP, CP, OP, P, P, P, P, P, ctypes.c_size_t, P]
     L.mmffb_fused_sd.restype = ctypes.c_int
     L.mmffb_fused_sd.argtypes = [BP, CP, OP, P, P, P, P]
+    L.mmffb_multimol_hist_floats.restype = ctypes.c_size_t
+    L.mmffb_multimol_hist_floats.argtypes = [CP, ctypes.c_int32]
+    L.mmffb_multimol_step.restype = ctypes.c_int
+    L.mmffb_multimol_step.argtypes = [BP, CP, ctypes.POINTER(MMFFMultiMolParams), ctypes.POINTER(MMFFMultiMolState),
+                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]
     L.mmffb_pack_chunk.restype = ctypes.c_int32
     L.mmffb_pack_chunk.argtypes = [ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_int32, P, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int

@@ -5,19 +5,20 @@ keep the reference signatures (mlxmolkit/mmff_metal_optimizer.py:217-225,
 543-548) and result types (:34-44, :210-214), plus an additive
 ``mmff_variant`` keyword (default "MMFF94", the reference's only variant).
 
-multi_mol: every conformer is minimised inside one persistent kernel launch
-(dense BFGS up to 150 atoms, L-BFGS with ``lbfgs_m`` pairs above) with the
-reference's convergence rule -- the largest per-atom norm of the gradient
-scaled by ``grad_scale`` at or below ``grad_tol``, tested every ``eval_freq``
-iterations (:334-359, :405-416).  Preserved behaviour:
-
-* ``converged[i] == (grad_norms[i] <= grad_tol)``, ``grad_norms`` being that
-  per-atom norm at the returned coordinates;
-* ``per_conf_iters`` is the iteration at which a conformer met ``grad_tol``
-  (``max_iters`` if it never did), so ``grad_tol=0`` gives ``max_iters``;
-* each conformer stops on its own, so raising ``max_iters`` past
-  convergence does not change the answer;
-* coordinates are written back into each molecule's conformers (:514-519).
+multi_mol runs the reference's own algorithm (:217-535) on the GPU:
+L-BFGS with ``lbfgs_m`` pairs on the ``grad_scale``-scaled gradient, no line
+search, each atom's step capped at ``max_step_per_atom``.  Every ``eval_freq``
+iterations it keeps the best-seen positions and marks the conformers whose
+largest per-atom scaled-gradient norm is at or below ``grad_tol``; the batch
+stops when all are.  It then returns every conformer to its best-seen
+positions and runs a polish pass of ``max_iters // 4`` iterations from a fresh
+history, stopping when every conformer is under ``grad_tol`` at a check point.
+The result holds the best-seen positions and their energies, the gradient
+norms of the last iterate, the iteration of each conformer's first passing
+check and the sticky converged flags of the main loop, as the reference's.
+The iterations run inside ``mmffb_multimol_step`` launches (one per
+``eval_freq`` iterations, state resident on the device); the host reads one
+counter per check point, where the reference synchronises too.
 
 The energies use the constants of the reference's mega kernel
 (mmff_metal_kernel.py:274-280), like the reference entry point.
@@ -28,6 +29,7 @@ zero and ``n_iters = max_iters`` as in the reference (:642-650).
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 from typing import Optional
 
@@ -87,14 +89,63 @@ def _write_back(mol, cids, xyz):
                 conf.SetAtomPosition(a, xyz[k, a].astype(float).tolist())
 
 
-def _atom_grad_norms(m: mm.Minimizer, positions: np.ndarray, grad_scale: float, mode) -> np.ndarray:
-    _, g = m.energy_grad(positions, precision="mixed", mode=mode)
-    out = np.empty(m.confs.n_conf)
-    for c in range(m.confs.n_conf):
-        n = int(m.params_list[m.conf_mol[c]].n_atoms)
-        gc = g[m.conf_coord[c]: m.conf_coord[c] + 3 * n].reshape(n, 3) * grad_scale
-        out[c] = np.sqrt((gc.astype(np.float64) ** 2).sum(1)).max() if n else 0.0
-    return out
+class _MultiMolRun:
+    """Device state of one multi-molecule L-BFGS run (the reference's loop variables)."""
+
+    def __init__(self, m: mm.Minimizer, pos: np.ndarray, lbfgs_m: int, grad_scale: float,
+                 max_step_per_atom: float, grad_tol: float, mode=mm.MODE_MEGA):
+        import torch
+        self.torch, self.m, self.L = torch, m, _lib.load()
+        dev = m.batch.device
+        C = m.confs.n_conf
+        self.hist_m = int(lbfgs_m)
+        if not 1 <= self.hist_m <= 16:
+            raise ValueError("lbfgs_m must be in 1..16")
+        self.x = torch.from_numpy(np.ascontiguousarray(pos, dtype=np.float32)).to(dev)
+        self.g = torch.zeros_like(self.x)
+        self.best_x = torch.zeros_like(self.x)
+        self.e = torch.zeros(C, dtype=torch.float64, device=dev)
+        self.best_e = torch.zeros_like(self.e)
+        self.bd, self.cd = m.batch.desc(), m.confs.desc()
+        hf = self.L.mmffb_multimol_hist_floats(ctypes.byref(self.cd), self.hist_m)
+        self.hist = torch.zeros(max(C * hf, 1), dtype=torch.float32, device=dev)
+        self.rho = torch.zeros(max(C * self.hist_m, 1), dtype=torch.float32, device=dev)
+        ints = lambda k: torch.zeros(max(k, 1), dtype=torch.int32, device=dev)
+        self.hcount, self.converged, self.conv_iter, self.pending = ints(C), ints(C), ints(C), ints(1)
+        self.state = _lib.MMFFMultiMolState(*(t.data_ptr() for t in (
+            self.x, self.g, self.best_x, self.e, self.best_e, self.hist, self.rho, self.hcount,
+            self.converged, self.conv_iter, self.pending)))
+        self.prm = _lib.MMFFMultiMolParams(self.hist_m, float(grad_scale), float(max_step_per_atom),
+                                           float(grad_tol), (ctypes.c_double * 4)(*mode))
+
+    def step(self, phase: int, n_iters: int = 0, it_end: int = 0, max_iters: int = 0) -> None:
+        rc = self.L.mmffb_multimol_step(ctypes.byref(self.bd), ctypes.byref(self.cd), ctypes.byref(self.prm),
+                                        ctypes.byref(self.state), phase, n_iters, it_end, max_iters,
+                                        ctypes.c_void_p(self.torch.cuda.current_stream().cuda_stream))
+        _lib.check(rc, "mmffb_multimol_step")
+
+    def _loop(self, total: int, eval_freq: int, check_phase: int, max_iters: int) -> int:
+        """Run ``total`` iterations in chunks ending at the check points (every eval_freq
+        iterations); returns the iteration count at which every conformer passed, or total."""
+        it = 0
+        while it < total:
+            n = min(eval_freq - it % eval_freq, total - it)
+            check = (it + n) % eval_freq == 0
+            if check:
+                self.pending.zero_()
+            self.step(check_phase if check else _lib.MM_RUN, n, it + n, max_iters)
+            it += n
+            if check and int(self.pending.item()) == 0:
+                return it
+        return total
+
+    def run(self, max_iters: int, eval_freq: int) -> int:
+        self.step(_lib.MM_START, 0, 0, max_iters)
+        iters_used = self._loop(max_iters, eval_freq, _lib.MM_MAIN_CHECK, max_iters)   # :346-410
+        self.step(_lib.MM_REVERT, 0, 0, max_iters)                                     # :412-428
+        self._loop(max_iters // 4, eval_freq, _lib.MM_POLISH_CHECK, max_iters)         # :430-483
+        self.torch.cuda.synchronize()
+        return iters_used
 
 
 def mmff_optimize_metal_multi_mol(
@@ -107,34 +158,32 @@ def mmff_optimize_metal_multi_mol(
     grad_tol: float = 1e-4,
     mmff_variant: str = "MMFF94",
 ) -> MultiMolResult:
-    """Optimise many molecules' conformers in one persistent GPU launch.
-
-    ``max_step_per_atom`` is accepted for signature compatibility; the line
-    search of the in-kernel optimizer controls the step length instead.
-    """
+    """Optimise many molecules' conformers with the reference's multi-molecule L-BFGS."""
+    if eval_freq < 1:
+        raise ValueError("eval_freq must be >= 1")
     mols, conf_ids, params, counts, pos = _collect(mol_specs, mmff_variant)
     m = mm.Minimizer(params, counts)
-    big = max(p.n_atoms for p in params) >= mm.LBFGS_ATOM_THRESHOLD
-    hist = max(1, min(int(lbfgs_m), 16)) if big else 0
-    r = m.minimize(pos, max_iters=max_iters, grad_tol=grad_tol, history_m=hist, mode=mm.MODE_MEGA,
-                   exit_test=_lib.EXIT_ATOM_NORM, check_every=max(1, int(eval_freq)),
-                   atom_grad_scale=grad_scale)
-    gn = _atom_grad_norms(m, r.positions, grad_scale, mm.MODE_MEGA)
-    conv = gn <= grad_tol
-    per_iters = np.where(conv, np.minimum(r.iters, max_iters), max_iters).astype(np.int32)
+    run = _MultiMolRun(m, pos, lbfgs_m, grad_scale, max_step_per_atom, grad_tol)
+    iters_used = run.run(int(max_iters), int(eval_freq))
+    best_x = run.best_x.cpu().numpy()
+    best_e = run.best_e.cpu().numpy()
+    g_last = run.g.cpu().numpy()
+    conv = run.converged.cpu().numpy()[: m.confs.n_conf].astype(bool)
+    per_iters = run.conv_iter.cpu().numpy()[: m.confs.n_conf].astype(np.int32)
     results, cursor = [], 0
     for mi, (mol, cids) in enumerate(zip(mols, conf_ids)):
         k = len(cids)
         n = int(params[mi].n_atoms)
         sl = slice(cursor, cursor + k)
         start = int(m.conf_coord[cursor])
-        xyz = r.positions[start: start + 3 * n * k].reshape(k, n, 3)
+        xyz = best_x[start: start + 3 * n * k].reshape(k, n, 3)
+        gl = g_last[start: start + 3 * n * k].reshape(k, n, 3).astype(np.float64)
+        gn = np.sqrt((gl * gl).sum(-1)).max(axis=1) if n else np.zeros(k)
         _write_back(mol, cids, xyz)
         results.append(MetalBatchResult(
-            energies=r.energies[sl].astype(np.float32), positions=xyz.copy(),
-            grad_norms=gn[sl].astype(np.float32),
-            n_iters=int(per_iters.max()) if conv.all() else int(max_iters), n_conformers=k,
-            per_conf_iters=per_iters[sl].copy(), converged=conv[sl].copy()))
+            energies=best_e[sl].astype(np.float32), positions=xyz.copy(), grad_norms=gn.astype(np.float32),
+            n_iters=int(iters_used), n_conformers=k, per_conf_iters=per_iters[sl].copy(),
+            converged=conv[sl].copy()))
         cursor += k
     return MultiMolResult(mol_results=results)
 

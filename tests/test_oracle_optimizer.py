@@ -46,3 +46,22 @@ def test_threads_do_not_change_results(golden):
     b = oracle.minimize(p, [3, 3, 3], pos, max_iters=300, n_threads=4)
     for u, v in zip(a, b):
         assert np.array_equal(u, v)
+
+
+def test_multimol_restatement_descends_and_records_convergence(golden):
+    from helpers import golden_mol
+    from mlxmolkit_b200.mmff_params import extract_mmff_params
+    from oracle import multimol
+    mols = [golden_mol(golden, mi) for mi in range(2)]
+    params = [extract_mmff_params(m) for m in mols]
+    counts = [m.GetNumConformers() for m in mols]
+    x0 = np.concatenate([np.stack([c.pos for c in m.GetConformers()]).reshape(-1) for m in mols])
+    r = multimol.multi_mol(params, counts, x0, max_iters=300, grad_tol=1e-3)
+    e0, o = [], 0
+    for p, k in zip(params, counts):
+        for _ in range(k):
+            e0.append(oracle.energy_grad(p, x0[o: o + 3 * p.n_atoms], mode=oracle.MODE_MEGA)[0])
+            o += 3 * p.n_atoms
+    assert np.all(r["energies"] <= np.array(e0) + 1e-9)
+    assert np.all(r["per_conf_iters"][r["converged"]] <= r["n_iters"])
+    assert r["n_iters"] % 10 == 0 or r["n_iters"] == 300
