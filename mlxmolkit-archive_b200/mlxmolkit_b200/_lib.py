@@ -55,9 +55,28 @@ class MMFFMultiMolParams(ctypes.Structure):
 
 MM_START, MM_REVERT, MM_RUN, MM_MAIN_CHECK, MM_POLISH_CHECK = 0, 1, 2, 3, 4
 
+
+class MMFFDGBatchDev(ctypes.Structure):
+    """include/mmffb200_dg.h: the distance-geometry stage's device batch."""
+    _fields_ = [("n_mols", ctypes.c_int32), ("n_conf", ctypes.c_int32), ("dim", ctypes.c_int32),
+                ("max_atoms", ctypes.c_int32)] + [
+        (f, P) for f in ("conf_to_mol", "conf_atom_starts", "conf_order", "mol_n_atoms", "mol_atom_base",
+                         "dist_starts", "dist_rec", "dinc_starts", "dinc_rec", "chiral_starts", "chiral_quads",
+                         "chiral_bounds", "cinc_starts", "cinc_rec", "fourth_count")]
+
+
+class MMFFDGParams(ctypes.Structure):
+    _fields_ = [("max_iters", ctypes.c_int32), ("lbfgs_m", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("grad_tol", ctypes.c_float), ("chiral_weight", ctypes.c_float),
+                ("fourth_dim_weight", ctypes.c_float)]
+
+
+DG_CONVERGED, DG_MAXIT = 0, 1
+
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step"]
+           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step",
+           "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad"]
 
 _lib = None
 
@@ -97,6 +116,13 @@ def load():
                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]
     L.mmffb_pack_chunk.restype = ctypes.c_int32
     L.mmffb_pack_chunk.argtypes = [ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_int32, P, P]
+    DBP, DPP = ctypes.POINTER(MMFFDGBatchDev), ctypes.POINTER(MMFFDGParams)
+    L.mmffb_dg_scratch_bytes.restype = ctypes.c_size_t
+    L.mmffb_dg_scratch_bytes.argtypes = [DBP, DPP]
+    L.mmffb_dg_minimize.restype = ctypes.c_int
+    L.mmffb_dg_minimize.argtypes = [DBP, DPP, P, P, P, P, P, ctypes.c_size_t, P]
+    L.mmffb_dg_energy_grad.restype = ctypes.c_int
+    L.mmffb_dg_energy_grad.argtypes = [DBP, DPP, P, P, P, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int
     L.mmffb_minimize_noalloc.argtypes = [BP, CP, OP, P, P, P, P, P, P]
     _lib = L

@@ -1,0 +1,187 @@
+"""Distance-geometry (DG) parameters per molecule, and the DG initial embedding.
+
+Mirror of the reference's mlxmolkit/dg_extract.py:
+  * ``DGParams`` (:20-53): the same fields;
+  * ``extract_dg_params`` (:173-283): the same rules that turn a distance-bounds
+    matrix into terms -- every pair i < j with positive bounds whose linear
+    spread ub - lb is at most 5 A, weight 1, squared bounds -- plus the fixed
+    signed chiral-volume windows ([5, 100], [2, 100] for 3-coordinate centres,
+    negated for the other handedness) and one fourth-dimension term per atom;
+  * ``metric_matrix_positions`` (:56-103): random distances within the bounds,
+    double-centred Gram matrix, top-``dim`` eigenvectors scaled by sqrt(lambda),
+    a uniform [-1, 1] column where an eigenvalue is not positive.  The random
+    draws are taken in the reference's order (one uniform per upper-triangle
+    pair, then the uniform columns), so a seed gives the reference's starts.
+
+RDKit is not available here, so the bounds matrix of RDKit's
+``GetMoleculeBoundsMatrix`` (which ``get_bounds_matrix`` wraps, :151-170) and
+its chiral tags have no source.  ``synth_bounds_matrix`` and
+``synth_chiral_tags`` are a synthetic stand-in for the seeded molecules of
+``synth.py``: bounds from the topology and the embedded conformer (tight 1-2
+and 1-3, a band for 1-4, van der Waals floors and path-length ceilings
+beyond), chirality from the conformer's signed volumes.  They give constraint
+sets of the reference's structure and size; they do not reproduce RDKit's
+numbers.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+# linear bound spread above which a pair is left out of the DG error function (dg_extract.py:203-207)
+BASIN_THRESH = 5.0
+
+
+@dataclass
+class DGParams:
+    """Distance-geometry terms of one molecule (dg_extract.py:20-53)."""
+    n_atoms: int
+    dist_idx1: np.ndarray
+    dist_idx2: np.ndarray
+    dist_lb2: np.ndarray
+    dist_ub2: np.ndarray
+    dist_weight: np.ndarray
+    chiral_idx1: np.ndarray
+    chiral_idx2: np.ndarray
+    chiral_idx3: np.ndarray
+    chiral_idx4: np.ndarray
+    chiral_vol_lower: np.ndarray
+    chiral_vol_upper: np.ndarray
+    fourth_idx: np.ndarray
+    bounds_mat: Optional[np.ndarray] = None
+
+
+CHI_CW, CHI_CCW, CHI_OTHER = "CW", "CCW", "OTHER"
+
+
+def extract_dg_params(mol, bounds_mat: np.ndarray, dim: int = 4, basin_size_tol: float = 1e8,
+                      chiral_tags: Optional[dict] = None) -> DGParams:
+    """DG terms from a bounds matrix (upper bounds above the diagonal, lower bounds below).
+
+    ``chiral_tags`` maps a centre atom to CW / CCW / OTHER; when it is None the
+    molecule's own ``chiral_tags`` attribute is used if it has one.
+    """
+    bm = np.asarray(bounds_mat, dtype=np.float64)
+    n = int(mol.GetNumAtoms())
+    iu, ju = np.triu_indices(n, 1)
+    ub, lb = bm[iu, ju], bm[ju, iu]
+    keep = (ub > 0) & (lb > 0) & ~(ub - lb > BASIN_THRESH)
+    iu, ju, ub, lb = iu[keep], ju[keep], ub[keep], lb[keep]
+
+    tags = chiral_tags if chiral_tags is not None else getattr(mol, "chiral_tags", None) or {}
+    quads, lo, hi = [], [], []
+    for center in sorted(tags):
+        nb = [a.GetIdx() for a in mol.GetAtomWithIdx(center).GetNeighbors()]
+        if len(nb) < 3:
+            continue
+        if len(nb) == 3:
+            q, lo_mag = (nb[0], nb[1], nb[2], center), 2.0
+        else:
+            q, lo_mag = (nb[0], nb[1], nb[2], nb[3]), 5.0
+        tag = tags[center]
+        if tag == CHI_CCW:
+            lo.append(lo_mag), hi.append(100.0)
+        elif tag == CHI_CW:
+            lo.append(-100.0), hi.append(-lo_mag)
+        else:
+            lo.append(-100.0), hi.append(100.0)
+        quads.append(q)
+    qa = np.array(quads, dtype=np.int32).reshape(-1, 4)
+    return DGParams(
+        n_atoms=n,
+        dist_idx1=iu.astype(np.int32), dist_idx2=ju.astype(np.int32),
+        dist_lb2=(lb * lb).astype(np.float32), dist_ub2=(ub * ub).astype(np.float32),
+        dist_weight=np.ones(len(iu), dtype=np.float32),
+        chiral_idx1=qa[:, 0].copy(), chiral_idx2=qa[:, 1].copy(), chiral_idx3=qa[:, 2].copy(),
+        chiral_idx4=qa[:, 3].copy(),
+        chiral_vol_lower=np.array(lo, dtype=np.float32), chiral_vol_upper=np.array(hi, dtype=np.float32),
+        fourth_idx=np.arange(n, dtype=np.int32),
+        bounds_mat=bm.astype(np.float32),
+    )
+
+
+def _metric_embed(bmat: np.ndarray, rng: np.random.Generator, dim: int) -> np.ndarray:
+    n = int(bmat.shape[0])
+    if n <= 1:
+        return np.zeros((n, dim), np.float32)
+    iu, ju = np.triu_indices(n, 1)
+    upper = bmat[iu, ju].astype(np.float64)
+    lower = np.minimum(bmat[ju, iu].astype(np.float64), upper)
+    d = lower + rng.random(len(upper)) * (upper - lower)
+    d2 = np.zeros((n, n))
+    d2[iu, ju] = d2[ju, iu] = d * d
+    gram = -0.5 * (d2 - d2.mean(axis=1, keepdims=True) - d2.mean(axis=0, keepdims=True) + d2.mean())
+    evals, evecs = np.linalg.eigh(gram)
+    top = np.argsort(evals)[::-1][:dim]
+    cols = [evecs[:, k] * np.sqrt(evals[k]) if evals[k] > 0.0 else 1.0 - 2.0 * rng.random(n) for k in top]
+    return np.stack(cols, axis=1).astype(np.float32)
+
+
+def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) -> np.ndarray:
+    """Metric-matrix initial coordinates of every conformer (flat, atom-major, float32)."""
+    rng = np.random.default_rng(seed)
+    starts = np.asarray(batch.conf_atom_starts)
+    out = np.zeros(int(starts[-1]) * dim, np.float32)
+    for c in range(int(batch.n_confs_total)):
+        a0, a1 = int(starts[c]), int(starts[c + 1])
+        bm = bounds_mats[int(batch.conf_to_mol[c])]
+        if bm is None:
+            out[a0 * dim:a1 * dim] = rng.standard_normal((a1 - a0) * dim).astype(np.float32)
+        else:
+            out[a0 * dim:a1 * dim] = _metric_embed(np.asarray(bm), rng, dim).reshape(-1)
+    return out
+
+
+# van der Waals radii (A) of the generator's elements, for the non-bonded lower bounds
+_VDW = {"H": 1.10, "C": 1.70, "N": 1.55, "O": 1.52, "F": 1.47, "S": 1.80, "Cl": 1.75, "Br": 1.85, "P": 1.80}
+
+
+def synth_bounds_matrix(mol, conf_id: int = 0) -> np.ndarray:
+    """Synthetic stand-in for RDKit's bounds matrix of a ``synth`` molecule (see the module doc)."""
+    pos = np.asarray(mol.GetConformer(conf_id).GetPositions(), dtype=np.float64)
+    n = len(pos)
+    dist = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    topo = np.asarray(mol.distance_matrix())
+    path = np.full((n, n), np.inf)
+    np.fill_diagonal(path, 0.0)
+    for b in mol.GetBonds():
+        i, j = b.GetBeginAtomIdx(), b.GetEndAtomIdx()
+        path[i, j] = path[j, i] = dist[i, j]
+    for k in range(n):                                   # shortest bond-path lengths (Floyd-Warshall)
+        path = np.minimum(path, path[:, k:k + 1] + path[k:k + 1, :])
+    rad = np.array([_VDW.get(a.GetSymbol(), 1.7) for a in mol.GetAtoms()])
+    lb = np.where(topo == 1, dist - 0.01,
+         np.where(topo == 2, dist - 0.04,
+         np.where(topo == 3, np.maximum(dist - 0.6, 2.0), 0.7 * (rad[:, None] + rad[None, :]))))
+    ub = np.where(topo == 1, dist + 0.01,
+         np.where(topo == 2, dist + 0.04,
+         np.where(topo == 3, dist + 0.6, np.maximum(path, dist + 0.1))))
+    lb = np.minimum(lb, dist)                            # the embedded conformer stays feasible
+    bm = np.zeros((n, n))
+    iu, ju = np.triu_indices(n, 1)
+    bm[iu, ju] = ub[iu, ju]
+    bm[ju, iu] = lb[iu, ju]
+    return bm
+
+
+def synth_chiral_tags(mol, conf_id: int = 0) -> dict:
+    """Chiral tags for a ``synth`` molecule: 4-coordinate centres with at most one hydrogen,
+    handedness from the embedded conformer's signed volume (positive = CCW window)."""
+    pos = np.asarray(mol.GetConformer(conf_id).GetPositions(), dtype=np.float64)
+    tags = {}
+    for a in mol.GetAtoms():
+        nb = [x.GetIdx() for x in a.GetNeighbors()]
+        if len(nb) != 4 or sum(mol.GetAtomWithIdx(k).GetSymbol() == "H" for k in nb) > 1:
+            continue
+        v1, v2, v3 = (pos[nb[k]] - pos[nb[3]] for k in range(3))
+        vol = float(np.dot(v1, np.cross(v2, v3)))
+        if abs(vol) >= 5.0:
+            tags[a.GetIdx()] = CHI_CCW if vol > 0 else CHI_CW
+    return tags
+
+
+def synth_dg_params(mol, conf_id: int = 0) -> DGParams:
+    """DG terms of a ``synth`` molecule: the stand-in bounds and tags through ``extract_dg_params``."""
+    return extract_dg_params(mol, synth_bounds_matrix(mol, conf_id), chiral_tags=synth_chiral_tags(mol, conf_id))

@@ -22,6 +22,12 @@ def golden():
     return np.load(os.path.join(ROOT, "tests", "golden", "ref_mmff_synth.npz"))
 
 
+@pytest.fixture(scope="session")
+def dg_golden():
+    import numpy as np
+    return np.load(os.path.join(ROOT, "tests", "golden", "ref_dg_batches.npz"))
+
+
 @pytest.fixture(scope="session", autouse=True)
 def _built_library():
     """Build libmmffb200.so (nvcc, sm_100a) once if a fresh checkout has none: the packer's

@@ -22,9 +22,25 @@ def install():
     chem.Mol = synth.SynthMol
     ff.MMFFGetMoleculeProperties = synth.MMFFGetMoleculeProperties
     chem.rdForceFieldHelpers = ff
+    # the distance-geometry modules: chirality read from a SynthMol's ``chiral_tags`` dict
+    # ({atom: "CW" | "CCW" | "OTHER"}), stereo assignment a no-op, rdDistGeom and mlx.core empty
+    chem.ChiralType = _ChiralType
+    chem.AssignStereochemistry = lambda mol, cleanIt=True, force=True: None
+    synth.SynthAtom.GetChiralTag = lambda atom: _ChiralType.BY_NAME.get(
+        (getattr(atom._mol, "chiral_tags", None) or {}).get(atom.GetIdx()), _ChiralType.CHI_UNSPECIFIED)
+    dg = types.ModuleType("rdkit.Chem.rdDistGeom")
+    chem.rdDistGeom = dg
     rdkit.Chem = chem
-    sys.modules.update({"rdkit": rdkit, "rdkit.Chem": chem, "rdkit.Chem.rdForceFieldHelpers": ff})
+    mlx = types.ModuleType("mlx")
+    mlx.core = types.ModuleType("mlx.core")
+    sys.modules.update({"rdkit": rdkit, "rdkit.Chem": chem, "rdkit.Chem.rdForceFieldHelpers": ff,
+                        "rdkit.Chem.rdDistGeom": dg, "mlx": mlx, "mlx.core": mlx.core})
     return rdkit
+
+
+class _ChiralType:
+    CHI_UNSPECIFIED, CHI_TETRAHEDRAL_CW, CHI_TETRAHEDRAL_CCW, CHI_OTHER = "unspec", "cw", "ccw", "other"
+    BY_NAME = {"CW": CHI_TETRAHEDRAL_CW, "CCW": CHI_TETRAHEDRAL_CCW, "OTHER": CHI_OTHER}
 
 
 def import_reference(ref_root: str):
