@@ -1,5 +1,6 @@
 /*
- * mmffb200_dg -- C ABI of the distance-geometry (DG) minimisation stage.
+ * mmffb200_dg -- C ABI of the embedding stages: distance geometry (DG) and the
+ * experimental-torsion (ETK) refinement.
  *
  * Same conventions as mmffb200.h (whose error codes, mmffb_stream_t and
  * mmffb_last_error() it shares; both are exported by libmmffb200.so): every
@@ -27,6 +28,18 @@
  *   cinc_rec       int32[2] {term index, role 0..3} listed under each of the
  *                  term's four atoms, rows as for dinc_rec
  *   fourth_count   int32 per atom row: how many fourth-dimension terms name it
+ *
+ * The ETK stage (mlxmolkit/etk_metal.py:27-536, replacing the kernel dispatch of
+ * etk_minimize_shared, :567-683) runs the same L-BFGS in 3-D without the first-gradient
+ * scaling on MMFFETKTermsDev terms (written by shared_batch.etk_device_arrays):
+ *   fb_rec         flat-bottom distance terms {i | j << 16, lb, ub, weight} (bounds in A):
+ *                  a molecule's 1-2, 1-3 and 1-4 terms; fbinc_rec lists them per atom as
+ *                  {other, lb, ub, weight}
+ *   tor_quads      int32[4] and tor_coef float32[12] {V0..V5, s0..s5} per 6-term Fourier
+ *                  torsion; a molecule's torsions, then its impropers (V1 = w, s1 = -1);
+ *                  tinc_rec lists them per atom as {term, role}
+ * The conformer map (conf_*, mol_n_atoms, mol_atom_base, dim = 3) comes from an
+ * MMFFDGBatchDev whose DG term pointers are not read.
  */
 #ifndef MMFFB200_DG_H
 #define MMFFB200_DG_H
@@ -67,6 +80,19 @@ typedef struct {
     float fourth_dim_weight;   /* weight of every fourth-dimension term */
 } MMFFDGParams;
 
+typedef struct {
+    int32_t max_tor;                 /* most Fourier terms (torsions + impropers) of one molecule */
+    const int32_t *fb_starts;        /* [n_mols + 1] */
+    const float *fb_rec;             /* [n_fb][4] */
+    const int32_t *fbinc_starts;     /* [n_atom_rows + 1] */
+    const float *fbinc_rec;          /* [2 * n_fb][4] */
+    const int32_t *tor_starts;       /* [n_mols + 1] */
+    const int32_t *tor_quads;        /* [n_tor][4] */
+    const float *tor_coef;           /* [n_tor][12] */
+    const int32_t *tinc_starts;      /* [n_atom_rows + 1] */
+    const int32_t *tinc_rec;         /* [4 * n_tor][2] */
+} MMFFETKTermsDev;
+
 /* Device scratch that mmffb_dg_minimize needs (L-BFGS histories of the resident CTAs + a work counter). */
 size_t mmffb_dg_scratch_bytes(const MMFFDGBatchDev *batch, const MMFFDGParams *params);
 
@@ -78,6 +104,15 @@ int mmffb_dg_minimize(const MMFFDGBatchDev *batch, const MMFFDGParams *params, f
 /* DG energy and unscaled gradient of every conformer at pos (grad has pos's layout). */
 int mmffb_dg_energy_grad(const MMFFDGBatchDev *batch, const MMFFDGParams *params, const float *pos,
                          float *energies, float *grad, mmffb_stream_t stream);
+
+/* The ETK stage: scratch, minimisation in place (params: max_iters, lbfgs_m, threads, grad_tol;
+ * the weights are not used), and energy + gradient.  confs->dim must be 3. */
+size_t mmffb_etk_scratch_bytes(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params);
+int mmffb_etk_minimize(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params,
+                       float *pos, float *energies, int32_t *statuses, int32_t *iters, void *scratch,
+                       size_t scratch_bytes, mmffb_stream_t stream);
+int mmffb_etk_energy_grad(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params,
+                          const float *pos, float *energies, float *grad, mmffb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -30,10 +30,17 @@
 //     reference evaluates the same function at the same point again (same code, same
 //     order), so the value is the same and the evaluation is skipped.
 //
+// The ETK stage (mlxmolkit/etk_metal.py:27-536) runs the same optimizer (FF = kETK) without the
+// first-gradient scaling, in 3-D, on 6-term Fourier torsions (impropers are Fourier terms with
+// V1 = w, s1 = -1) and flat-bottom 1-2 / 1-3 / 1-4 distance terms.  Its gradient has two
+// phases: every Fourier term writes its four atoms' gradient vectors to shared memory, then
+// each thread sums, for its own atoms, those rows and its flat-bottom incidences.
+//
 // No wait in this file spins: every loop is bounded by the iteration caps.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "mmffb200_dg.h"
 
@@ -51,8 +58,11 @@ constexpr float kMaxStepFactor = 100.0f;  // :35
 constexpr int kMaxLs = 1000;              // :36
 constexpr int kMaxHist = 16;
 
+constexpr int kDG = 0, kETK = 1;
+
 struct Args {
     MMFFDGBatchDev b;
+    MMFFETKTermsDev e;
     MMFFDGParams p;
     float *pos;
     float *energy;
@@ -62,6 +72,7 @@ struct Args {
     float4 *hist;
     int *counter;
     int slot_atoms;
+    int tor_slots;   // Fourier-term gradient rows in shared memory (ETK)
 };
 
 template <int NT>
@@ -255,6 +266,168 @@ __device__ void dg_gradient(const Args &a, const float4 *X, float4 *G, int mol, 
     }
 }
 
+// ---------------------------------------------------------------- ETK terms
+
+__device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct Tors {
+    float3 r1, r2, r3, r4, t0, t1;
+};
+
+// the reference's torsion convention: r1 = p1 - p2, r2 = p3 - p2, r3 = -r2, r4 = p4 - p3,
+// normals t0 = r1 x r2, t1 = r3 x r4 (etk_metal.py:35-49)
+__device__ __forceinline__ Tors tors_geom(float4 p1, float4 p2, float4 p3, float4 p4) {
+    Tors T;
+    T.r1 = sub3(xyz(p1), xyz(p2));
+    T.r2 = sub3(xyz(p3), xyz(p2));
+    T.r3 = make_float3(-T.r2.x, -T.r2.y, -T.r2.z);
+    T.r4 = sub3(xyz(p4), xyz(p3));
+    T.t0 = cross3(T.r1, T.r2);
+    T.t1 = cross3(T.r3, T.r4);
+    return T;
+}
+
+// cos(phi) as the energy takes it: 0 for a degenerate pair of normals, clamped to [-1, 1]
+__device__ __forceinline__ float tors_cos(const Tors &T) {
+    const float comb = dot3(T.t0, T.t0) * dot3(T.t1, T.t1);
+    if (comb < 1e-16f) return 0.0f;
+    return fminf(fmaxf(dot3(T.t0, T.t1) * rsqrtf(comb), -1.0f), 1.0f);
+}
+
+struct Coef {
+    float V[6], S[6];
+};
+
+__device__ __forceinline__ Coef load_coef(const float *coef, int t) {
+    const float4 *c = reinterpret_cast<const float4 *>(coef) + 3 * (size_t)t;
+    const float4 a = __ldg(c), b = __ldg(c + 1), d = __ldg(c + 2);
+    Coef k;
+    k.V[0] = a.x; k.V[1] = a.y; k.V[2] = a.z; k.V[3] = a.w; k.V[4] = b.x; k.V[5] = b.y;
+    k.S[0] = b.z; k.S[1] = b.w; k.S[2] = d.x; k.S[3] = d.y; k.S[4] = d.z; k.S[5] = d.w;
+    return k;
+}
+
+// sum_k V_k (1 + s_k T_{k+1}(c)) with T_n the Chebyshev polynomials (T_n(cos phi) = cos(n phi)),
+// and d/dc of it (etk_metal.py:51-61)
+__device__ __forceinline__ float fourier(float c, const Coef &k, float *dedc) {
+    float t0 = 1.0f, t1 = c, d0 = 0.0f, d1 = 1.0f, e = 0.0f, de = 0.0f;
+#pragma unroll
+    for (int n = 1; n <= 6; ++n) {
+        e += k.V[n - 1] * (1.0f + k.S[n - 1] * t1);
+        de += k.V[n - 1] * k.S[n - 1] * d1;
+        const float t2 = 2.0f * c * t1 - t0, d2 = 2.0f * t1 + 2.0f * c * d1 - d0;
+        t0 = t1; t1 = t2; d0 = d1; d1 = d2;
+    }
+    if (dedc) *dedc = de;
+    return e;
+}
+
+// gradient of one Fourier term on its four atoms: dE/dcos through the two cross products;
+// zero when a normal is degenerate (etk_metal.py:63-103 keeps the same cases)
+__device__ __forceinline__ void tors_grad(const Tors &T, const Coef &k, float3 g[4]) {
+    const float d0 = dot3(T.t0, T.t0), d1 = dot3(T.t1, T.t1);
+    if (d0 < 1e-16f || d1 < 1e-16f) {
+        g[0] = g[1] = g[2] = g[3] = make_float3(0.f, 0.f, 0.f);
+        return;
+    }
+    const float i0 = rsqrtf(fmaxf(d0, 1e-16f)), i1 = rsqrtf(fmaxf(d1, 1e-16f));
+    const float3 n0 = make_float3(T.t0.x * i0, T.t0.y * i0, T.t0.z * i0);
+    const float3 n1 = make_float3(T.t1.x * i1, T.t1.y * i1, T.t1.z * i1);
+    const float c = fminf(fmaxf(dot3(n0, n1), -1.0f), 1.0f);
+    const float sp = sqrtf(fmaxf(1.0f - c * c, 0.0f));
+    float dedc;
+    fourier(c, k, &dedc);
+    const float dedphi = -sp * dedc;
+    const float st = fabsf(sp) > 1e-8f ? -dedphi / sp : -dedphi / fmaxf(fabsf(c), 1e-16f) * (c + 1e-30f >= 0.f ? 1.f : -1.f);
+    const float3 dc0 = make_float3(i0 * (n1.x - c * n0.x), i0 * (n1.y - c * n0.y), i0 * (n1.z - c * n0.z));
+    const float3 dc1 = make_float3(i1 * (n0.x - c * n1.x), i1 * (n0.y - c * n1.y), i1 * (n0.z - c * n1.z));
+    const float3 a1 = cross3(T.r2, dc0), a2 = cross3(dc0, T.r1), a3 = cross3(T.r4, dc1), a4 = cross3(dc1, T.r3);
+    g[0] = make_float3(st * a1.x, st * a1.y, st * a1.z);
+    g[1] = make_float3(st * (a3.x - a1.x - a2.x), st * (a3.y - a1.y - a2.y), st * (a3.z - a1.z - a2.z));
+    g[2] = make_float3(st * (a2.x - a3.x - a4.x), st * (a2.y - a3.y - a4.y), st * (a2.z - a3.z - a4.z));
+    g[3] = make_float3(st * a4.x, st * a4.y, st * a4.z);
+}
+
+// flat-bottom term: w (d - bound)^2 outside [lb, ub], d = sqrt(d^2 + 1e-12) (etk_metal.py:126-150)
+__device__ __forceinline__ float fb_e(float4 xi, float4 xj, float lb, float ub, float w) {
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float dist = sqrtf(dx * dx + dy * dy + dz * dz + 1e-12f);
+    if (dist < lb) return w * (dist - lb) * (dist - lb);
+    if (dist > ub) return w * (dist - ub) * (dist - ub);
+    return 0.0f;
+}
+
+template <int NT>
+__device__ float etk_energy(const Args &a, const float4 *X, int mol, float *buf) {
+    const MMFFETKTermsDev &E = a.e;
+    const float4 *rec = reinterpret_cast<const float4 *>(E.fb_rec);
+    float e = 0.0f;
+    const int f1 = E.fb_starts[mol + 1];
+    for (int t = E.fb_starts[mol] + (int)threadIdx.x; t < f1; t += NT) {
+        const float4 r = __ldg(rec + t);
+        const int ij = __float_as_int(r.x);
+        e += fb_e(X[ij & 0xffff], X[ij >> 16], r.y, r.z, r.w);
+    }
+    const int4 *quads = reinterpret_cast<const int4 *>(E.tor_quads);
+    const int t1 = E.tor_starts[mol + 1];
+    for (int t = E.tor_starts[mol] + (int)threadIdx.x; t < t1; t += NT) {
+        const int4 q = __ldg(quads + t);
+        e += fourier(tors_cos(tors_geom(X[q.x], X[q.y], X[q.z], X[q.w])), load_coef(E.tor_coef, t), nullptr);
+    }
+    return bsum<NT>(e, buf);
+}
+
+template <int NT>
+__device__ void etk_gradient(const Args &a, const float4 *X, float4 *G, int mol, int N, int base, float4 *TG) {
+    const MMFFETKTermsDev &E = a.e;
+    const int4 *quads = reinterpret_cast<const int4 *>(E.tor_quads);
+    const int ts = E.tor_starts[mol], te = E.tor_starts[mol + 1];
+    for (int t = ts + (int)threadIdx.x; t < te; t += NT) {
+        const int4 q = __ldg(quads + t);
+        float3 g[4];
+        tors_grad(tors_geom(X[q.x], X[q.y], X[q.z], X[q.w]), load_coef(E.tor_coef, t), g);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) TG[4 * (t - ts) + r] = make_float4(g[r].x, g[r].y, g[r].z, 0.f);
+    }
+    bar<NT>();
+    const float4 *inc = reinterpret_cast<const float4 *>(E.fbinc_rec);
+    const int2 *tinc = reinterpret_cast<const int2 *>(E.tinc_rec);
+    for (int i = threadIdx.x; i < N; i += NT) {
+        const int r = base + i;
+        const float4 xi = X[i];
+        float gx = 0.f, gy = 0.f, gz = 0.f;
+        const int e1 = __ldg(E.fbinc_starts + r + 1);
+        for (int k = __ldg(E.fbinc_starts + r); k < e1; ++k) {
+            const float4 q = __ldg(inc + k);
+            const float4 xo = X[__float_as_int(q.x)];
+            const float dx = xi.x - xo.x, dy = xi.y - xo.y, dz = xi.z - xo.z;
+            const float dist = sqrtf(dx * dx + dy * dy + dz * dz + 1e-12f);
+            float pf = 0.0f;
+            if (dist < q.y) pf = q.w * 2.0f * (dist - q.y) / dist;
+            else if (dist > q.z) pf = q.w * 2.0f * (dist - q.z) / dist;
+            gx += pf * dx;
+            gy += pf * dy;
+            gz += pf * dz;
+        }
+        const int k1 = __ldg(E.tinc_starts + r + 1);
+        for (int k = __ldg(E.tinc_starts + r); k < k1; ++k) {
+            const int2 tr = __ldg(tinc + k);
+            const float4 v = TG[4 * (tr.x - ts) + tr.y];
+            gx += v.x;
+            gy += v.y;
+            gz += v.z;
+        }
+        G[i] = make_float4(gx, gy, gz, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------- the optimizer
+
 __device__ __forceinline__ float4 load_atom(const float *P, int i, int dim) {
     if (dim == 4) return make_float4(P[4 * i], P[4 * i + 1], P[4 * i + 2], P[4 * i + 3]);
     return make_float4(P[3 * i], P[3 * i + 1], P[3 * i + 2], 0.0f);
@@ -275,8 +448,21 @@ __device__ __forceinline__ float4 axpy(float a, float4 x, float4 y) {  // y + a 
 __device__ __forceinline__ float4 scale4(float a, float4 x) { return f4(a * x.x, a * x.y, a * x.z, a * x.w); }
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) { return f4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__ Args a) {
+template <int NT, int FF>
+__device__ __forceinline__ float ff_energy(const Args &a, const float4 *X, int mol, int N, int base, float *buf) {
+    if constexpr (FF == kDG) return dg_energy<NT>(a, X, mol, N, base, buf);
+    else return etk_energy<NT>(a, X, mol, buf);
+}
+
+template <int NT, int FF>
+__device__ __forceinline__ void ff_gradient(const Args &a, const float4 *X, float4 *G, int mol, int N, int base,
+                                            float4 *TG) {
+    if constexpr (FF == kDG) dg_gradient<NT>(a, X, G, mol, N, base);
+    else etk_gradient<NT>(a, X, G, mol, N, base, TG);
+}
+
+template <int NT, int FF>
+__global__ void __launch_bounds__(NT) lbfgs_kernel(const __grid_constant__ Args a) {
     constexpr int NW = NT / 32;
     extern __shared__ float4 sm[];
     __shared__ int s_next;
@@ -284,6 +470,7 @@ __global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__
     float4 *X = sm, *G = X + NA, *D = G + NA, *XO = D + NA, *GO = XO + NA, *Q = GO + NA;
     float *rbase = reinterpret_cast<float *>(Q + NA);
     float *rho = rbase + 2 * NW * 4;
+    float4 *TG = reinterpret_cast<float4 *>(rho + kMaxHist);
     int rsel = 0;
     auto rb = [&]() {
         rsel ^= 1;
@@ -305,15 +492,17 @@ __global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__
         for (int i = tid; i < N; i += NT) X[i] = load_atom(P, i, dim);
         bar<NT>();
 
-        float energy = dg_energy<NT>(a, X, mol, N, base, rb());
-        dg_gradient<NT>(a, X, G, mol, N, base);
-        // 0.1 scaling, halved while max > 10 (conformer_metal.py:303-313)
-        for (int i = tid; i < N; i += NT) G[i] = scale4(0.1f, G[i]);
-        for (int sc = 0; sc < 20; ++sc) {
-            float mx = 0.f;
-            for (int i = tid; i < N; i += NT) mx = fmaxf(mx, amax4(G[i]));
-            if (bmax<NT>(mx, rb()) <= 10.0f) break;
-            for (int i = tid; i < N; i += NT) G[i] = scale4(0.5f, G[i]);
+        float energy = ff_energy<NT, FF>(a, X, mol, N, base, rb());
+        ff_gradient<NT, FF>(a, X, G, mol, N, base, TG);
+        if constexpr (FF == kDG) {
+            // 0.1 scaling, halved while max > 10 (conformer_metal.py:303-313); ETK has none
+            for (int i = tid; i < N; i += NT) G[i] = scale4(0.1f, G[i]);
+            for (int sc = 0; sc < 20; ++sc) {
+                float mx = 0.f;
+                for (int i = tid; i < N; i += NT) mx = fmaxf(mx, amax4(G[i]));
+                if (bmax<NT>(mx, rb()) <= 10.0f) break;
+                for (int i = tid; i < N; i += NT) G[i] = scale4(0.5f, G[i]);
+            }
         }
         float ss = 0.f;
         for (int i = tid; i < N; i += NT) {
@@ -355,7 +544,7 @@ __global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__
                 }
                 for (int i = tid; i < N; i += NT) X[i] = axpy(lam, D[i], XO[i]);
                 bar<NT>();
-                const float te = dg_energy<NT>(a, X, mol, N, base, rb());
+                const float te = ff_energy<NT, FF>(a, X, mol, N, base, rb());
                 if (te - old_e <= kFuncTol * lam * slope) {
                     energy = te;
                     done = true;
@@ -400,7 +589,7 @@ __global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__
                 break;
             }
             for (int i = tid; i < N; i += NT) GO[i] = G[i];
-            dg_gradient<NT>(a, X, G, mol, N, base);
+            ff_gradient<NT, FF>(a, X, G, mol, N, base, TG);
             float gt = 0.f;
             for (int i = tid; i < N; i += NT) {
                 const float4 g = G[i], x = X[i];
@@ -472,22 +661,22 @@ __global__ void __launch_bounds__(NT) dg_minimize_kernel(const __grid_constant__
     }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) dg_energy_grad_kernel(const __grid_constant__ Args a) {
+template <int NT, int FF>
+__global__ void __launch_bounds__(NT) energy_grad_kernel(const __grid_constant__ Args a) {
     constexpr int NW = NT / 32;
     extern __shared__ float4 sm[];
     const int NA = a.slot_atoms;
     float4 *X = sm, *G = X + NA;
     float *red = reinterpret_cast<float *>(G + NA);
+    float4 *TG = reinterpret_cast<float4 *>(red + 2 * NW * 4 + kMaxHist);
     const MMFFDGBatchDev &b = a.b;
     const int c = blockIdx.x, dim = b.dim;
     const int mol = b.conf_to_mol[c], N = b.mol_n_atoms[mol], base = b.mol_atom_base[mol];
     const float *P = a.pos + (size_t)b.conf_atom_starts[c] * dim;
     for (int i = threadIdx.x; i < N; i += NT) X[i] = load_atom(P, i, dim);
     bar<NT>();
-    const float e = dg_energy<NT>(a, X, mol, N, base, red);
-    (void)NW;
-    dg_gradient<NT>(a, X, G, mol, N, base);
+    const float e = ff_energy<NT, FF>(a, X, mol, N, base, red);
+    ff_gradient<NT, FF>(a, X, G, mol, N, base, TG);
     float *GP = a.grad_out + (size_t)b.conf_atom_starts[c] * dim;
     for (int i = threadIdx.x; i < N; i += NT) store_atom(GP, i, dim, G[i]);
     if (threadIdx.x == 0) a.energy[c] = e;
@@ -498,12 +687,39 @@ int pick_threads(int max_atoms, int req) {
     return max_atoms <= 48 ? 32 : max_atoms <= 96 ? 64 : max_atoms <= 192 ? 128 : 256;
 }
 
-size_t smem_bytes(int nt, int na, int vectors) {
-    return (size_t)vectors * na * sizeof(float4) + (size_t)2 * (nt / 32) * 4 * sizeof(float) + kMaxHist * sizeof(float);
+// shared memory of a CTA: `vectors` float4 vectors of na atoms, the reduction halves, the
+// L-BFGS rho values and (ETK) four gradient rows per Fourier term
+size_t smem_bytes(int nt, int na, int vectors, int tor_slots) {
+    return (size_t)vectors * na * sizeof(float4) + (size_t)2 * (nt / 32) * 4 * sizeof(float) +
+           kMaxHist * sizeof(float) + (size_t)4 * tor_slots * sizeof(float4);
 }
 
-int check(const MMFFDGBatchDev *b, const MMFFDGParams *p) {
-    if (!b || !p) return fail(MMFFB_EINVAL, "null DG batch or parameters");
+template <int FF>
+const void *minimize_kernel_ff(int nt) {
+    switch (nt) {
+        case 32: return reinterpret_cast<const void *>(&lbfgs_kernel<32, FF>);
+        case 64: return reinterpret_cast<const void *>(&lbfgs_kernel<64, FF>);
+        case 128: return reinterpret_cast<const void *>(&lbfgs_kernel<128, FF>);
+        default: return reinterpret_cast<const void *>(&lbfgs_kernel<256, FF>);
+    }
+}
+
+const void *minimize_kernel_for(int nt, int ff) { return ff == kDG ? minimize_kernel_ff<kDG>(nt) : minimize_kernel_ff<kETK>(nt); }
+
+template <int FF>
+const void *energy_kernel_ff(int nt) {
+    switch (nt) {
+        case 32: return reinterpret_cast<const void *>(&energy_grad_kernel<32, FF>);
+        case 64: return reinterpret_cast<const void *>(&energy_grad_kernel<64, FF>);
+        case 128: return reinterpret_cast<const void *>(&energy_grad_kernel<128, FF>);
+        default: return reinterpret_cast<const void *>(&energy_grad_kernel<256, FF>);
+    }
+}
+
+const void *energy_kernel_for(int nt, int ff) { return ff == kDG ? energy_kernel_ff<kDG>(nt) : energy_kernel_ff<kETK>(nt); }
+
+int check_confs(const MMFFDGBatchDev *b, const MMFFDGParams *p) {
+    if (!b || !p) return fail(MMFFB_EINVAL, "null batch or parameters");
     if (b->n_conf < 0 || b->n_mols < 0) return fail(MMFFB_EINVAL, "negative count");
     if (b->dim != 3 && b->dim != 4) return fail(MMFFB_EINVAL, "dim must be 3 or 4, got %d", b->dim);
     if (b->n_conf > 0 && (b->max_atoms < 1 || b->max_atoms > 1024))
@@ -512,40 +728,70 @@ int check(const MMFFDGBatchDev *b, const MMFFDGParams *p) {
     if (p->max_iters < 0) return fail(MMFFB_EINVAL, "negative max_iters");
     if (p->threads != 0 && p->threads != 32 && p->threads != 64 && p->threads != 128 && p->threads != 256)
         return fail(MMFFB_EINVAL, "threads must be 0, 32, 64, 128 or 256");
-    if (b->n_conf > 0 && (!b->conf_to_mol || !b->conf_atom_starts || !b->mol_n_atoms || !b->mol_atom_base ||
-                          !b->dist_starts || !b->dinc_starts || !b->chiral_starts || !b->cinc_starts ||
+    if (b->n_conf > 0 && (!b->conf_to_mol || !b->conf_atom_starts || !b->mol_n_atoms || !b->mol_atom_base))
+        return fail(MMFFB_EINVAL, "null device pointer in the conformer map");
+    return 0;
+}
+
+int check(const MMFFDGBatchDev *b, const MMFFDGParams *p) {
+    int r = check_confs(b, p);
+    if (r) return r;
+    if (b->n_conf > 0 && (!b->dist_starts || !b->dinc_starts || !b->chiral_starts || !b->cinc_starts ||
                           !b->fourth_count))
         return fail(MMFFB_EINVAL, "null device pointer in DG batch");
     return 0;
 }
 
-template <int NT>
-const void *minimize_fn() { return reinterpret_cast<const void *>(&dg_minimize_kernel<NT>); }
-
-const void *minimize_kernel_for(int nt) {
-    switch (nt) {
-        case 32: return minimize_fn<32>();
-        case 64: return minimize_fn<64>();
-        case 128: return minimize_fn<128>();
-        default: return minimize_fn<256>();
-    }
+int check_etk(const MMFFDGBatchDev *b, const MMFFETKTermsDev *e, const MMFFDGParams *p) {
+    int r = check_confs(b, p);
+    if (r) return r;
+    if (!e) return fail(MMFFB_EINVAL, "null ETK terms");
+    if (b->dim != 3) return fail(MMFFB_EINVAL, "the ETK stage is 3-D, got dim %d", b->dim);
+    if (e->max_tor < 0 || e->max_tor > 8192) return fail(MMFFB_ETOOBIG, "max_tor %d outside 0..8192", e->max_tor);
+    if (b->n_conf > 0 && (!e->fb_starts || !e->fbinc_starts || !e->tor_starts || !e->tinc_starts))
+        return fail(MMFFB_EINVAL, "null device pointer in ETK terms");
+    return 0;
 }
 
-// resident CTAs of the minimise kernel on this device (the grid and the history slots)
-int plan_grid(const MMFFDGBatchDev *b, const MMFFDGParams *p, int *nt_out, size_t *smem_out, int *grid_out) {
-    const int nt = pick_threads(b->max_atoms, p->threads);
-    const size_t smem = smem_bytes(nt, b->max_atoms, 6);
-    const void *fn = minimize_kernel_for(nt);
+// resident CTAs per SM of the minimise kernel with nt threads
+int occupancy(int nt, int ff, int max_atoms, int tor_slots, int *occ, size_t *smem_out) {
+    const size_t smem = smem_bytes(nt, max_atoms, 6, tor_slots);
+    const void *fn = minimize_kernel_for(nt, ff);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(DG)");
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(L-BFGS)");
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, nt, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor(L-BFGS)");
+    *smem_out = smem;
+    return 0;
+}
+
+// Threads per conformer, grid and shared memory of a launch.  Unless the caller fixes the
+// thread count: the largest instance whose resident CTAs hold every conformer at once (a
+// batch too small to fill the GPU finishes when its slowest conformer does, so more threads
+// per conformer pay), else the size-based default (measured on B200: 1000 conformers of
+// <= 77 atoms 8.9k / 15.6k / 18.1k / 18.9k conformers/s at 32 / 64 / 128 / 256 threads;
+// 10000 conformers of <= 87 atoms 55k / 70k / 52k / 37k).
+int plan_grid(const MMFFDGBatchDev *b, const MMFFDGParams *p, int ff, int tor_slots, int *nt_out, size_t *smem_out,
+              int *grid_out) {
     int dev = 0, sms = 0, occ = 0;
-    e = cudaGetDevice(&dev);
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nt, smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor(DG)");
-    if (occ < 1) return fail(MMFFB_ETOOBIG, "DG kernel does not fit an SM (%zu B shared memory)", smem);
+    int nt = pick_threads(b->max_atoms, p->threads);
+    size_t smem = 0;
+    if (p->threads == 0)
+        for (int cand = 256; cand > nt; cand /= 2) {
+            int r = occupancy(cand, ff, b->max_atoms, tor_slots, &occ, &smem);
+            if (r) return r;
+            if (occ >= 1 && (long long)sms * occ >= b->n_conf) {
+                nt = cand;
+                break;
+            }
+        }
+    int r = occupancy(nt, ff, b->max_atoms, tor_slots, &occ, &smem);
+    if (r) return r;
+    if (occ < 1) return fail(MMFFB_ETOOBIG, "the L-BFGS kernel does not fit an SM (%zu B shared memory)", smem);
     long long g = (long long)sms * occ;
     if (g > b->n_conf) g = b->n_conf;
     *nt_out = nt;
@@ -555,6 +801,80 @@ int plan_grid(const MMFFDGBatchDev *b, const MMFFDGParams *p, int *nt_out, size_
 }
 
 constexpr size_t kCounterBytes = 256;
+
+size_t scratch_for(const MMFFDGBatchDev *b, const MMFFDGParams *p, int grid) {
+    return kCounterBytes + (size_t)grid * 2 * p->lbfgs_m * b->max_atoms * sizeof(float4);
+}
+
+int minimize(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGParams *p, int ff, float *pos,
+             float *energies, int32_t *statuses, int32_t *iters, void *scratch, size_t scratch_bytes,
+             mmffb_stream_t stream) {
+    if (b->n_conf == 0) return 0;
+    if (!pos || !energies || !statuses) return fail(MMFFB_EINVAL, "null output pointer");
+    const int tor_slots = ff == kETK ? etk->max_tor : 0;
+    int nt = 0, grid = 0;
+    size_t smem = 0;
+    int r = plan_grid(b, p, ff, tor_slots, &nt, &smem, &grid);
+    if (r) return r;
+    const size_t need = scratch_for(b, p, grid);
+    if (!scratch || scratch_bytes < need)
+        return fail(MMFFB_ESCRATCH, "scratch of %zu B given, %zu B needed", scratch_bytes, need);
+    Args a;
+    memset(&a, 0, sizeof a);
+    a.b = *b;
+    if (etk) a.e = *etk;
+    a.p = *p;
+    a.pos = pos;
+    a.energy = energies;
+    a.status = statuses;
+    a.iters = iters;
+    a.counter = reinterpret_cast<int *>(scratch);
+    a.hist = reinterpret_cast<float4 *>(reinterpret_cast<char *>(scratch) + kCounterBytes);
+    a.slot_atoms = b->max_atoms;
+    a.tor_slots = tor_slots;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(L-BFGS counter)");
+    void *args[] = {&a};
+    e = cudaLaunchKernel(minimize_kernel_for(nt, ff), dim3(grid), dim3(nt), args, smem, st);
+    if (e != cudaSuccess) return cuda_fail(e, "lbfgs_kernel launch");
+    return 0;
+}
+
+int energy_grad(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGParams *p, int ff, const float *pos,
+                float *energies, float *grad, mmffb_stream_t stream) {
+    if (b->n_conf == 0) return 0;
+    if (!pos || !energies || !grad) return fail(MMFFB_EINVAL, "null argument");
+    const int nt = pick_threads(b->max_atoms, p->threads);
+    const int tor_slots = ff == kETK ? etk->max_tor : 0;
+    const size_t smem = smem_bytes(nt, b->max_atoms, 2, tor_slots);
+    Args a;
+    memset(&a, 0, sizeof a);
+    a.b = *b;
+    if (etk) a.e = *etk;
+    a.p = *p;
+    a.pos = const_cast<float *>(pos);
+    a.energy = energies;
+    a.grad_out = grad;
+    a.slot_atoms = b->max_atoms;
+    a.tor_slots = tor_slots;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const void *fn = energy_kernel_for(nt, ff);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(energy)");
+    void *args[] = {&a};
+    e = cudaLaunchKernel(fn, dim3(b->n_conf), dim3(nt), args, smem, st);
+    if (e != cudaSuccess) return cuda_fail(e, "energy_grad_kernel launch");
+    return 0;
+}
+
+size_t scratch_bytes(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGParams *p, int ff) {
+    if (b->n_conf == 0) return kCounterBytes;
+    int nt = 0, grid = 0;
+    size_t smem = 0;
+    if (plan_grid(b, p, ff, ff == kETK ? etk->max_tor : 0, &nt, &smem, &grid)) return 0;
+    return scratch_for(b, p, grid);
+}
 
 }  // namespace dg
 }  // namespace mmffb
@@ -566,94 +886,41 @@ extern "C" {
 
 size_t mmffb_dg_scratch_bytes(const MMFFDGBatchDev *batch, const MMFFDGParams *params) {
     if (check(batch, params)) return 0;
-    if (batch->n_conf == 0) return kCounterBytes;
-    int nt = 0, grid = 0;
-    size_t smem = 0;
-    if (plan_grid(batch, params, &nt, &smem, &grid)) return 0;
-    return kCounterBytes + (size_t)grid * 2 * params->lbfgs_m * batch->max_atoms * sizeof(float4);
+    return scratch_bytes(batch, nullptr, params, kDG);
 }
 
 int mmffb_dg_minimize(const MMFFDGBatchDev *batch, const MMFFDGParams *params, float *pos, float *energies,
                       int32_t *statuses, int32_t *iters, void *scratch, size_t scratch_bytes, mmffb_stream_t stream) {
     int r = check(batch, params);
     if (r) return r;
-    if (batch->n_conf == 0) return 0;
-    if (!pos || !energies || !statuses) return fail(MMFFB_EINVAL, "null output pointer");
-    int nt = 0, grid = 0;
-    size_t smem = 0;
-    r = plan_grid(batch, params, &nt, &smem, &grid);
-    if (r) return r;
-    const size_t need = kCounterBytes + (size_t)grid * 2 * params->lbfgs_m * batch->max_atoms * sizeof(float4);
-    if (!scratch || scratch_bytes < need)
-        return fail(MMFFB_ESCRATCH, "DG scratch of %zu B given, %zu B needed", scratch_bytes, need);
-    Args a;
-    a.b = *batch;
-    a.p = *params;
-    a.pos = pos;
-    a.energy = energies;
-    a.status = statuses;
-    a.iters = iters;
-    a.grad_out = nullptr;
-    a.counter = reinterpret_cast<int *>(scratch);
-    a.hist = reinterpret_cast<float4 *>(reinterpret_cast<char *>(scratch) + kCounterBytes);
-    a.slot_atoms = batch->max_atoms;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(DG counter)");
-    switch (nt) {
-        case 32: dg_minimize_kernel<32><<<grid, 32, smem, st>>>(a); break;
-        case 64: dg_minimize_kernel<64><<<grid, 64, smem, st>>>(a); break;
-        case 128: dg_minimize_kernel<128><<<grid, 128, smem, st>>>(a); break;
-        default: dg_minimize_kernel<256><<<grid, 256, smem, st>>>(a); break;
-    }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "dg_minimize_kernel launch");
-    return 0;
+    return minimize(batch, nullptr, params, kDG, pos, energies, statuses, iters, scratch, scratch_bytes, stream);
 }
 
 int mmffb_dg_energy_grad(const MMFFDGBatchDev *batch, const MMFFDGParams *params, const float *pos, float *energies,
                          float *grad, mmffb_stream_t stream) {
     int r = check(batch, params);
     if (r) return r;
-    if (batch->n_conf == 0) return 0;
-    if (!pos || !energies || !grad) return fail(MMFFB_EINVAL, "null argument");
-    const int nt = pick_threads(batch->max_atoms, params->threads);
-    const size_t smem = smem_bytes(nt, batch->max_atoms, 2);
-    Args a;
-    a.b = *batch;
-    a.p = *params;
-    a.pos = const_cast<float *>(pos);
-    a.energy = energies;
-    a.status = nullptr;
-    a.iters = nullptr;
-    a.grad_out = grad;
-    a.hist = nullptr;
-    a.counter = nullptr;
-    a.slot_atoms = batch->max_atoms;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaSuccess;
-    switch (nt) {
-        case 32:
-            e = cudaFuncSetAttribute(dg_energy_grad_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) dg_energy_grad_kernel<32><<<batch->n_conf, 32, smem, st>>>(a);
-            break;
-        case 64:
-            e = cudaFuncSetAttribute(dg_energy_grad_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) dg_energy_grad_kernel<64><<<batch->n_conf, 64, smem, st>>>(a);
-            break;
-        case 128:
-            e = cudaFuncSetAttribute(dg_energy_grad_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) dg_energy_grad_kernel<128><<<batch->n_conf, 128, smem, st>>>(a);
-            break;
-        default:
-            e = cudaFuncSetAttribute(dg_energy_grad_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) dg_energy_grad_kernel<256><<<batch->n_conf, 256, smem, st>>>(a);
-            break;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(DG energy)");
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "dg_energy_grad_kernel launch");
-    return 0;
+    return energy_grad(batch, nullptr, params, kDG, pos, energies, grad, stream);
+}
+
+size_t mmffb_etk_scratch_bytes(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params) {
+    if (check_etk(confs, terms, params)) return 0;
+    return scratch_bytes(confs, terms, params, kETK);
+}
+
+int mmffb_etk_minimize(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params,
+                       float *pos, float *energies, int32_t *statuses, int32_t *iters, void *scratch,
+                       size_t scratch_bytes, mmffb_stream_t stream) {
+    int r = check_etk(confs, terms, params);
+    if (r) return r;
+    return minimize(confs, terms, params, kETK, pos, energies, statuses, iters, scratch, scratch_bytes, stream);
+}
+
+int mmffb_etk_energy_grad(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params,
+                          const float *pos, float *energies, float *grad, mmffb_stream_t stream) {
+    int r = check_etk(confs, terms, params);
+    if (r) return r;
+    return energy_grad(confs, terms, params, kETK, pos, energies, grad, stream);
 }
 
 }  // extern "C"

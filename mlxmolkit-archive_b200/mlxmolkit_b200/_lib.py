@@ -71,12 +71,20 @@ class MMFFDGParams(ctypes.Structure):
                 ("fourth_dim_weight", ctypes.c_float)]
 
 
+class MMFFETKTermsDev(ctypes.Structure):
+    """include/mmffb200_dg.h: the ETK stage's terms."""
+    _fields_ = [("max_tor", ctypes.c_int32)] + [
+        (f, P) for f in ("fb_starts", "fb_rec", "fbinc_starts", "fbinc_rec", "tor_starts", "tor_quads", "tor_coef",
+                         "tinc_starts", "tinc_rec")]
+
+
 DG_CONVERGED, DG_MAXIT = 0, 1
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
            "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step",
-           "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad"]
+           "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad",
+           "mmffb_etk_scratch_bytes", "mmffb_etk_minimize", "mmffb_etk_energy_grad"]
 
 _lib = None
 
@@ -123,6 +131,13 @@ def load():
     L.mmffb_dg_minimize.argtypes = [DBP, DPP, P, P, P, P, P, ctypes.c_size_t, P]
     L.mmffb_dg_energy_grad.restype = ctypes.c_int
     L.mmffb_dg_energy_grad.argtypes = [DBP, DPP, P, P, P, P]
+    ETP = ctypes.POINTER(MMFFETKTermsDev)
+    L.mmffb_etk_scratch_bytes.restype = ctypes.c_size_t
+    L.mmffb_etk_scratch_bytes.argtypes = [DBP, ETP, DPP]
+    L.mmffb_etk_minimize.restype = ctypes.c_int
+    L.mmffb_etk_minimize.argtypes = [DBP, ETP, DPP, P, P, P, P, P, ctypes.c_size_t, P]
+    L.mmffb_etk_energy_grad.restype = ctypes.c_int
+    L.mmffb_etk_energy_grad.argtypes = [DBP, ETP, DPP, P, P, P, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int
     L.mmffb_minimize_noalloc.argtypes = [BP, CP, OP, P, P, P, P, P, P]
     _lib = L

@@ -3,7 +3,10 @@
 The stage as ``generate_conformers_nk`` runs it (mlxmolkit/conformer_pipeline_v2.py:172-221):
 metric-matrix starts, the 4-D minimisation with the automatic iteration budget
 max(300, 300 + 20 * max_atoms) (fourth-dimension weight 0.1, chiral weight 1.0),
-then the 4-D -> 3-D collapse of 200 iterations (weights 1.0 / 0.2).  Inputs are
+then the 4-D -> 3-D collapse of 200 iterations (weights 1.0 / 0.2).  The ETK leg
+continues from there as the pipeline's stage 3 (:260-290): the first three
+coordinates, then ``etk_minimize_shared``'s kernel with the budget
+max(150, 150 + 10 * max_atoms) (the reference's "DG + ETK" rows).  Inputs are
 seeded synthetic molecules (heavy atoms 10-30; bounds and chirality from
 ``dg_extract.synth_dg_params``); the reference quotes its DG-only throughput on
 20 molecules x 50 conformers (docs/BENCHMARKS.md:44-50), and 1000 x 10 is its
@@ -16,11 +19,12 @@ Per workload it reports:
   * ``e2e_conf_per_s``: the same through ``dg_minimize_shared`` with host arrays
     (tables packed and uploaded, positions copied both ways, every call);
   * ``converged``: the fraction of conformers with status 0 after the 4-D stage;
+  * ``dg_etk_conf_per_s``: DG, collapse, 3-D extraction and ETK, all on the device;
   * ``oracle``: agreement with the FP64 oracle on a sample of conformers
     (statuses, and energies where both converged) and the oracle's own
     conformers/s on all host threads.
 
-Usage: python -m mlxmolkit_b200.dg_bench [--workloads 20x50,1000x10] [--cpu-sample 64]
+Usage: python -m mlxmolkit_b200.dg_bench [--workloads 20x50,1000x10] [--cpu-sample 64] [--tpm auto|32,64,...]
 """
 from __future__ import annotations
 
@@ -34,7 +38,9 @@ import numpy as np
 from . import synth
 from .conformer_metal import DGDeviceBatch, dg_minimize_shared
 from .dg_extract import metric_matrix_positions, synth_dg_params
-from .shared_batch import pack_shared_dg_batch
+from .etk_extract import synth_etk_params
+from .etk_metal import ETKDeviceBatch
+from .shared_batch import add_etk_to_batch, pack_shared_dg_batch
 
 
 def _auto_iters(max_atoms: int, base: int, scale: float) -> int:
@@ -48,7 +54,9 @@ def _workload(n_mols: int, k: int, seed: int):
     x0 = metric_matrix_positions(b4, [p.bounds_mat for p in params], seed=42, dim=4)
     max_atoms = max(p.n_atoms for p in params)
     complexity = max(max_atoms, int(max(len(p.dist_idx1) for p in params) ** 0.5))
-    return b4, x0, _auto_iters(complexity, 300, 20.0), max_atoms
+    b3 = pack_shared_dg_batch(params, [k] * n_mols, dim=3)
+    add_etk_to_batch(b3, [synth_etk_params(m, p.bounds_mat) for m, p in zip(mols, params)])
+    return b4, x0, _auto_iters(complexity, 300, 20.0), max_atoms, b3, _auto_iters(complexity, 150, 10.0)
 
 
 def _sub_batch(b, confs):
@@ -69,13 +77,13 @@ def _sub_batch(b, confs):
     return pack_shared_dg_batch(ps, counts, dim=b.dim), ordered
 
 
-def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0) -> dict:
+def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=None) -> dict:
     import torch
-    b4, x0, iters, max_atoms = _workload(n_mols, k, seed)
+    b4, x0, iters, max_atoms, b3, etk_iters = _workload(n_mols, k, seed)
     C = b4.n_confs_total
     dev = DGDeviceBatch(b4)
-    p1 = dev.params(iters, 1e-4, 1.0, 0.1)
-    p2 = dev.params(200, 1e-4, 0.2, 1.0)
+    p1 = dev.params(iters, 1e-4, 1.0, 0.1, tpm=tpm)
+    p2 = dev.params(200, 1e-4, 0.2, 1.0, tpm=tpm)
     start = torch.from_numpy(x0).cuda()
     pos = torch.empty_like(start)
     it = torch.empty(C, dtype=torch.int32, device="cuda")
@@ -107,15 +115,42 @@ def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0) -> di
     for _ in range(max(1, repeats // 2)):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        xa, _, _ = dg_minimize_shared(b4, x0, max_iters=iters, chiral_weight=1.0, fourth_dim_weight=0.1)
-        dg_minimize_shared(b4, xa, max_iters=200, chiral_weight=0.2, fourth_dim_weight=1.0)
+        xa, _, _ = dg_minimize_shared(b4, x0, max_iters=iters, chiral_weight=1.0, fourth_dim_weight=0.1, tpm=tpm)
+        dg_minimize_shared(b4, xa, max_iters=200, chiral_weight=0.2, fourth_dim_weight=1.0, tpm=tpm)
         e2e.append(time.perf_counter() - t)
     t_e2e = float(np.median(e2e))
 
+    # DG + ETK on the device: the 3-D start is the collapsed 4-D result's first three coordinates
+    edev = ETKDeviceBatch(b3)
+    p3 = edev.params(etk_iters, 1e-4, 0.0, 0.0, tpm=tpm)
+    it3 = torch.empty(C, dtype=torch.int32, device="cuda")
+
+    def dg_etk():
+        stage()
+        pos3 = pos.view(-1, 4)[:, :3].contiguous().view(-1)
+        e3, s3 = edev.minimize_device(pos3, p3, iters=it3)
+        return e3, s3
+
+    dg_etk()
+    times = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(st)
+        e3, s3 = dg_etk()
+        ev1.record(st)
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1) / 1e3)
+    t_dg_etk = float(np.median(times))
+    s3n, it3n = s3.cpu().numpy(), it3.cpu().numpy()
+
     out = {"workload": f"{n_mols}x{k} synthetic, heavy atoms 10-30", "conformers": C, "max_atoms": max_atoms,
+           "threads_per_conformer": tpm or "auto",
            "dg_max_iters": iters, "seconds": t_dev, "conf_per_s": C / t_dev, "ms_per_conf": t_dev * 1e3 / C,
            "e2e_seconds": t_e2e, "e2e_conf_per_s": C / t_e2e, "converged": float(np.mean(s1n == 0)),
-           "mean_iters": float(itn.mean()), "max_iters_hit": int(np.sum(itn >= iters))}
+           "mean_iters": float(itn.mean()), "max_iters_hit": int(np.sum(itn >= iters)),
+           "etk_max_iters": etk_iters, "dg_etk_seconds": t_dg_etk, "dg_etk_conf_per_s": C / t_dg_etk,
+           "etk_converged": float(np.mean(s3n == 0)), "etk_mean_iters": float(it3n.mean())}
     if cpu_sample:
         from oracle import dg as odg
         rng = np.random.default_rng(1)
@@ -142,12 +177,13 @@ def main():
     ap.add_argument("--workloads", default="20x50,1000x10")
     ap.add_argument("--repeats", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--tpm", default="auto", help="threads per conformer: auto or a comma list of 32/64/128/256")
     a = ap.parse_args()
-    res = []
+    tpms = [None] if a.tpm == "auto" else [int(v) for v in a.tpm.split(",")]
     for w in a.workloads.split(","):
         n, k = (int(v) for v in w.split("x"))
-        res.append(run(n, k, a.repeats, a.cpu_sample))
-        print(json.dumps(res[-1]), flush=True)
+        for tpm in tpms:
+            print(json.dumps(run(n, k, a.repeats, a.cpu_sample, tpm=tpm)), flush=True)
 
 
 if __name__ == "__main__":

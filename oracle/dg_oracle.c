@@ -27,6 +27,15 @@
  * and dist_bounds (t*3: lb^2, ub^2, weight); chiral_quads (t*4) and
  * chiral_bounds (t*2: lower, upper); fourth_idx (local atom indices).
  * Statuses: 0 converged (TOLX or gradient), 1 iteration cap reached.
+ *
+ * The ETK stage (mlxmolkit/etk_metal.py) runs the same L-BFGS (:353-536) without the
+ * first-gradient scaling, in 3-D, on
+ *   torsion preferences    E = sum_k V_k (1 + s_k cos((k+1) phi)), k = 0..5  (:51-61)
+ *   impropers              the same form with V = (0, w, 0...), s = (0, -1, 0...)  (:105-124)
+ *   1-2 / 1-3 / 1-4 terms  flat-bottom w (d - bound)^2 outside [lb, ub], d = sqrt(d^2 + 1e-12)  (:126-150)
+ * with cos(phi) from the normals of (p1-p2, p3-p2) and (p2-p3, p4-p3), 0 when their
+ * product is degenerate (:35-49).  The torsion gradient here is derived independently:
+ * dE/dcos through the two cross products.
  */
 #include <math.h>
 #include <pthread.h>
@@ -50,13 +59,159 @@ typedef struct {
     const int32_t *fourth_term_starts, *fourth_idx;
 } DGOBatch;
 
+/* ETK terms in the reference kernel's layout (etk_metal.py:609-650): torsions (quads, V[6],
+ * signs[6]), impropers (quads, weight), and three flat-bottom lists (pairs, {lb, ub, w}). */
+typedef struct {
+    const int32_t *tor_starts, *tor_quads;
+    const float *tor_V, *tor_signs;
+    const int32_t *imp_starts, *imp_quads;
+    const float *imp_w;
+    const int32_t *fb_starts[3], *fb_pairs[3];
+    const float *fb_bounds[3];
+} ETKOTerms;
+
 typedef struct {
     const DGOBatch *b;
     int mol, n, dim;
     double chiral_w, fourth_w;
+    const ETKOTerms *etk; /* NULL: the DG error function */
 } Sys;
 
+/* cos(phi) of the reference's torsion convention; ok = 0 where the energy treats it as 0 */
+static double tors_cos(const double *x, int dim, const int *q, double t0[3], double t1[3], double r[4][3]) {
+    for (int d = 0; d < 3; ++d) {
+        r[0][d] = x[q[0] * dim + d] - x[q[1] * dim + d];
+        r[1][d] = x[q[2] * dim + d] - x[q[1] * dim + d];
+        r[2][d] = -r[1][d];
+        r[3][d] = x[q[3] * dim + d] - x[q[2] * dim + d];
+    }
+    t0[0] = r[0][1] * r[1][2] - r[0][2] * r[1][1];
+    t0[1] = r[0][2] * r[1][0] - r[0][0] * r[1][2];
+    t0[2] = r[0][0] * r[1][1] - r[0][1] * r[1][0];
+    t1[0] = r[2][1] * r[3][2] - r[2][2] * r[3][1];
+    t1[1] = r[2][2] * r[3][0] - r[2][0] * r[3][2];
+    t1[2] = r[2][0] * r[3][1] - r[2][1] * r[3][0];
+    const double comb = (t0[0] * t0[0] + t0[1] * t0[1] + t0[2] * t0[2]) * (t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    if (comb < 1e-16) return 0.0;
+    double c = (t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2]) / sqrt(comb);
+    return c < -1.0 ? -1.0 : c > 1.0 ? 1.0 : c;
+}
+
+/* sum_k V_k (1 + s_k T_{k+1}(c)) and its derivative in c (Chebyshev T_n(cos phi) = cos(n phi)) */
+static double fourier(double c, const double *V, const double *s, double *dedc) {
+    double T[8], dT[8];
+    T[0] = 1.0; T[1] = c; dT[0] = 0.0; dT[1] = 1.0;
+    for (int n = 2; n <= 6; ++n) {
+        T[n] = 2.0 * c * T[n - 1] - T[n - 2];
+        dT[n] = 2.0 * T[n - 1] + 2.0 * c * dT[n - 1] - dT[n - 2];
+    }
+    double e = 0.0, de = 0.0;
+    for (int k = 0; k < 6; ++k) {
+        e += V[k] * (1.0 + s[k] * T[k + 1]);
+        de += V[k] * s[k] * dT[k + 1];
+    }
+    if (dedc) *dedc = de;
+    return e;
+}
+
+static void cross3(const double a[3], const double b[3], double o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* gradient of one Fourier torsion term added into g (the reference's degenerate cases kept) */
+static void tors_grad(const double *x, int dim, const int *q, const double *V, const double *s, double *g) {
+    double t0[3], t1[3], r[4][3];
+    tors_cos(x, dim, q, t0, t1, r);
+    const double d0 = t0[0] * t0[0] + t0[1] * t0[1] + t0[2] * t0[2], d1 = t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2];
+    if (d0 < 1e-16 || d1 < 1e-16) return;
+    const double i0 = 1.0 / sqrt(d0), i1 = 1.0 / sqrt(d1);
+    double n0[3], n1[3];
+    for (int d = 0; d < 3; ++d) { n0[d] = t0[d] * i0; n1[d] = t1[d] * i1; }
+    double c = n0[0] * n1[0] + n0[1] * n1[1] + n0[2] * n1[2];
+    c = c < -1.0 ? -1.0 : c > 1.0 ? 1.0 : c;
+    const double sp = sqrt(fmax(1.0 - c * c, 0.0));
+    double dedc;
+    fourier(c, V, s, &dedc);
+    const double dedphi = -sp * dedc;
+    const double st = fabs(sp) > 1e-8 ? -dedphi / sp : -dedphi / fmax(fabs(c), 1e-16) * (c + 1e-30 >= 0 ? 1.0 : -1.0);
+    double dc0[3], dc1[3]; /* d cos / d t0, d cos / d t1 */
+    for (int d = 0; d < 3; ++d) {
+        dc0[d] = i0 * (n1[d] - c * n0[d]);
+        dc1[d] = i1 * (n0[d] - c * n1[d]);
+    }
+    /* t0 = r1 x r2, t1 = r3 x r4: df/da = b x df/dt, df/db = df/dt x a */
+    double a1[3], a2[3], a3[3], a4[3];
+    cross3(r[1], dc0, a1); /* d/d r1 */
+    cross3(dc0, r[0], a2); /* d/d r2 */
+    cross3(r[3], dc1, a3); /* d/d r3 */
+    cross3(dc1, r[2], a4); /* d/d r4 */
+    for (int d = 0; d < 3; ++d) {
+        g[q[0] * dim + d] += st * a1[d];                      /* r1 = p1 - p2 */
+        g[q[1] * dim + d] += st * (-a1[d] - a2[d] + a3[d]);   /* r1, r2 = p3 - p2, r3 = p2 - p3 */
+        g[q[2] * dim + d] += st * (a2[d] - a3[d] - a4[d]);    /* r2, r3, r4 = p4 - p3 */
+        g[q[3] * dim + d] += st * a4[d];
+    }
+}
+
+static const double kImpS[6] = {0, -1, 0, 0, 0, 0};
+
+static double etk_energy(const Sys *s, const double *x) {
+    const ETKOTerms *T = s->etk;
+    const int m = s->mol, dim = s->dim;
+    double e = 0.0, t0[3], t1[3], r[4][3], V[6], sg[6];
+    for (int t = T->tor_starts[m]; t < T->tor_starts[m + 1]; ++t) {
+        for (int k = 0; k < 6; ++k) { V[k] = T->tor_V[6 * t + k]; sg[k] = T->tor_signs[6 * t + k]; }
+        e += fourier(tors_cos(x, dim, T->tor_quads + 4 * t, t0, t1, r), V, sg, NULL);
+    }
+    for (int t = T->imp_starts[m]; t < T->imp_starts[m + 1]; ++t) {
+        const double Vi[6] = {0, T->imp_w[t], 0, 0, 0, 0};
+        e += fourier(tors_cos(x, dim, T->imp_quads + 4 * t, t0, t1, r), Vi, kImpS, NULL);
+    }
+    for (int l = 0; l < 3; ++l)
+        for (int t = T->fb_starts[l][m]; t < T->fb_starts[l][m + 1]; ++t) {
+            const int a = T->fb_pairs[l][2 * t], b = T->fb_pairs[l][2 * t + 1];
+            const double lb = T->fb_bounds[l][3 * t], ub = T->fb_bounds[l][3 * t + 1], w = T->fb_bounds[l][3 * t + 2];
+            double d2 = 0.0;
+            for (int d = 0; d < 3; ++d) { const double df = x[a * dim + d] - x[b * dim + d]; d2 += df * df; }
+            const double dist = sqrt(d2 + 1e-12);
+            if (dist < lb) e += w * (dist - lb) * (dist - lb);
+            else if (dist > ub) e += w * (dist - ub) * (dist - ub);
+        }
+    return e;
+}
+
+static void etk_grad(const Sys *s, const double *x, double *g) {
+    const ETKOTerms *T = s->etk;
+    const int m = s->mol, dim = s->dim;
+    memset(g, 0, sizeof(double) * (size_t)s->n * dim);
+    double V[6], sg[6];
+    for (int t = T->tor_starts[m]; t < T->tor_starts[m + 1]; ++t) {
+        for (int k = 0; k < 6; ++k) { V[k] = T->tor_V[6 * t + k]; sg[k] = T->tor_signs[6 * t + k]; }
+        tors_grad(x, dim, T->tor_quads + 4 * t, V, sg, g);
+    }
+    for (int t = T->imp_starts[m]; t < T->imp_starts[m + 1]; ++t) {
+        const double Vi[6] = {0, T->imp_w[t], 0, 0, 0, 0};
+        tors_grad(x, dim, T->imp_quads + 4 * t, Vi, kImpS, g);
+    }
+    for (int l = 0; l < 3; ++l)
+        for (int t = T->fb_starts[l][m]; t < T->fb_starts[l][m + 1]; ++t) {
+            const int a = T->fb_pairs[l][2 * t], b = T->fb_pairs[l][2 * t + 1];
+            const double lb = T->fb_bounds[l][3 * t], ub = T->fb_bounds[l][3 * t + 1], w = T->fb_bounds[l][3 * t + 2];
+            double df[3], d2 = 0.0;
+            for (int d = 0; d < 3; ++d) { df[d] = x[a * dim + d] - x[b * dim + d]; d2 += df[d] * df[d]; }
+            const double dist = sqrt(d2 + 1e-12);
+            double pf = 0.0;
+            if (dist < lb) pf = w * 2.0 * (dist - lb) / dist;
+            else if (dist > ub) pf = w * 2.0 * (dist - ub) / dist;
+            if (pf != 0.0)
+                for (int d = 0; d < 3; ++d) { g[a * dim + d] += pf * df[d]; g[b * dim + d] -= pf * df[d]; }
+        }
+}
+
 static double sys_energy(const Sys *s, const double *x) {
+    if (s->etk) return etk_energy(s, x);
     const DGOBatch *b = s->b;
     const int dim = s->dim, m = s->mol;
     double e = 0.0;
@@ -99,6 +254,7 @@ static double sys_energy(const Sys *s, const double *x) {
 }
 
 static void sys_grad(const Sys *s, const double *x, double *g) {
+    if (s->etk) { etk_grad(s, x, g); return; }
     const DGOBatch *b = s->b;
     const int dim = s->dim, m = s->mol;
     memset(g, 0, sizeof(double) * (size_t)s->n * dim);
@@ -170,12 +326,14 @@ static int minimize_one(const Sys *s, double *x, int max_iters, double grad_tol,
 
     double energy = sys_energy(s, x);
     sys_grad(s, x, g);
-    for (int i = 0; i < nv; ++i) g[i] *= 0.1;
-    for (int sc = 0; sc < 20; ++sc) {
-        double mx = 0.0;
-        for (int i = 0; i < nv; ++i) mx = dmax(mx, fabs(g[i]));
-        if (mx <= 10.0) break;
-        for (int i = 0; i < nv; ++i) g[i] *= 0.5;
+    if (!s->etk) { /* the DG stage scales its first gradient; ETK does not (etk_metal.py:353) */
+        for (int i = 0; i < nv; ++i) g[i] *= 0.1;
+        for (int sc = 0; sc < 20; ++sc) {
+            double mx = 0.0;
+            for (int i = 0; i < nv; ++i) mx = dmax(mx, fabs(g[i]));
+            if (mx <= 10.0) break;
+            for (int i = 0; i < nv; ++i) g[i] *= 0.5;
+        }
     }
     for (int i = 0; i < nv; ++i) dir[i] = -g[i];
     double ss = 0.0;
@@ -307,15 +465,16 @@ static int minimize_one(const Sys *s, double *x, int max_iters, double grad_tol,
 }
 
 /* energy and gradient of one conformer at x (double, the conformer's n*dim coordinates) */
-double dg_oracle_energy_grad(const DGOBatch *b, int conf, const double *x, double chiral_w, double fourth_w,
-                             double *grad) {
-    Sys s = {b, b->conf_to_mol[conf], b->mol_n_atoms[b->conf_to_mol[conf]], b->dim, chiral_w, fourth_w};
+double dg_oracle_energy_grad(const DGOBatch *b, const ETKOTerms *etk, int conf, const double *x, double chiral_w,
+                             double fourth_w, double *grad) {
+    Sys s = {b, b->conf_to_mol[conf], b->mol_n_atoms[b->conf_to_mol[conf]], b->dim, chiral_w, fourth_w, etk};
     if (grad) sys_grad(&s, x, grad);
     return sys_energy(&s, x);
 }
 
 typedef struct {
     const DGOBatch *b;
+    const ETKOTerms *etk;
     const float *pos_in;
     double *pos_out, *energies;
     int32_t *statuses, *iters;
@@ -337,7 +496,7 @@ static void *worker(void *arg) {
         const size_t off = (size_t)b->conf_atom_starts[c] * dim;
         double *x = J->pos_out + off;
         for (int i = 0; i < n * dim; ++i) x[i] = J->pos_in[off + i];
-        Sys s = {b, m, n, dim, J->chiral_w, J->fourth_w};
+        Sys s = {b, m, n, dim, J->chiral_w, J->fourth_w, J->etk};
         int it = 0;
         J->statuses[c] = minimize_one(&s, x, J->max_iters, J->grad_tol, J->M, &J->energies[c], &it);
         if (J->iters) J->iters[c] = it;
@@ -346,12 +505,14 @@ static void *worker(void *arg) {
 }
 
 /* all conformers of the batch on n_threads host threads; pos_out in double */
-int dg_oracle_minimize(const DGOBatch *b, const float *pos_in, double *pos_out, double *energies, int32_t *statuses,
-                       int32_t *iters, int max_iters, double grad_tol, double chiral_w, double fourth_w, int lbfgs_m,
-                       int n_threads) {
-    if (!b || !pos_in || !pos_out || !energies || !statuses || lbfgs_m < 1 || (b->dim != 3 && b->dim != 4))
+/* etk = NULL: the DG stage; otherwise the ETK stage (dim must be 3) */
+int dg_oracle_minimize(const DGOBatch *b, const ETKOTerms *etk, const float *pos_in, double *pos_out, double *energies,
+                       int32_t *statuses, int32_t *iters, int max_iters, double grad_tol, double chiral_w,
+                       double fourth_w, int lbfgs_m, int n_threads) {
+    if (!b || !pos_in || !pos_out || !energies || !statuses || lbfgs_m < 1 || (b->dim != 3 && b->dim != 4) ||
+        (etk && b->dim != 3))
         return -1;
-    Job J = {b, pos_in, pos_out, energies, statuses, iters, max_iters, lbfgs_m, grad_tol, chiral_w, fourth_w, 0,
+    Job J = {b, etk, pos_in, pos_out, energies, statuses, iters, max_iters, lbfgs_m, grad_tol, chiral_w, fourth_w, 0,
              PTHREAD_MUTEX_INITIALIZER};
     if (n_threads < 1) n_threads = 1;
     pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)n_threads);

@@ -13,6 +13,8 @@ the REFERENCE's own mlxmolkit/dg_extract.py (``extract_dg_params``,
     (tests/test_conformer_metal.py:22-43), and
   * seeded synthetic molecules whose bounds matrix and chiral tags come from
     this package's stand-ins (``synth_bounds_matrix``, ``synth_chiral_tags``),
+    and their ETK terms (``etk_extract.synth_etk_params``) through the
+    reference's ``add_etk_to_batch`` (mlxmolkit/shared_batch.py:204-296),
 
 and stores the inputs and the reference's outputs in
 ``tests/golden/ref_dg_batches.npz``.  The tests compare this package's
@@ -34,10 +36,17 @@ sys.path.insert(0, HERE)
 import fake_rdkit  # noqa: E402
 from mlxmolkit_b200 import synth  # noqa: E402
 from mlxmolkit_b200.dg_extract import synth_bounds_matrix, synth_chiral_tags  # noqa: E402
+from mlxmolkit_b200.etk_extract import synth_etk_params  # noqa: E402
 
 BATCH_FIELDS = ("conf_atom_starts", "conf_to_mol", "mol_n_atoms", "dist_idx1", "dist_idx2", "dist_lb2", "dist_ub2",
                 "dist_weight", "dist_term_starts", "chiral_idx1", "chiral_idx2", "chiral_idx3", "chiral_idx4",
                 "chiral_vol_lower", "chiral_vol_upper", "chiral_term_starts", "fourth_idx", "fourth_term_starts")
+ETK_FIELDS = ("torsion_idx", "torsion_V", "torsion_signs", "improper_idx", "improper_weight", "dist12_idx1",
+              "dist12_idx2", "dist12_lb", "dist12_ub", "dist12_weight", "dist13_idx1", "dist13_idx2", "dist13_lb",
+              "dist13_ub", "dist13_weight", "dist14_idx1", "dist14_idx2", "dist14_lb", "dist14_ub", "dist14_weight")
+ETK_BATCH = ["etk_torsion_idx", "etk_torsion_V", "etk_torsion_signs", "etk_torsion_term_starts", "etk_improper_idx",
+             "etk_improper_weight", "etk_improper_term_starts"] + [
+    f"etk_dist{t}_{f}" for t in ("12", "13", "14") for f in ("idx1", "idx2", "lb", "ub", "weight", "term_starts")]
 PARAM_FIELDS = ("dist_idx1", "dist_idx2", "dist_lb2", "dist_ub2", "dist_weight", "chiral_idx1", "chiral_idx2",
                 "chiral_idx3", "chiral_idx4", "chiral_vol_lower", "chiral_vol_upper", "fourth_idx")
 # (seed, heavy_lo, heavy_hi) of the synthetic molecules, and their conformer counts
@@ -65,6 +74,7 @@ def main(ref_root: str) -> None:
         sys.path.insert(0, ref_root)
     rdg = importlib.import_module("mlxmolkit.dg_extract")
     rsb = importlib.import_module("mlxmolkit.shared_batch")
+    retk = importlib.import_module("mlxmolkit.etk_extract")
     out = {}
 
     # all-pairs sets of the reference's tests
@@ -75,7 +85,7 @@ def main(ref_root: str) -> None:
     out["ap_init_seed7"] = rsb.init_random_positions(b, seed=7)
 
     # synthetic molecules through the reference's extraction
-    params, bms = [], []
+    params, bms, etks = [], [], []
     for mi, (seed, lo, hi) in enumerate(SYNTH):
         rng = np.random.default_rng(seed)
         mol = synth.generate_molecule(rng, lo, hi, name=f"dg-golden-{mi}")
@@ -97,12 +107,20 @@ def main(ref_root: str) -> None:
             out[pre + "ref_" + f] = np.asarray(getattr(p, f))
         params.append(p)
         bms.append(bm)
+        ep = synth_etk_params(mol, bm)
+        for f in ETK_FIELDS:
+            out[pre + "etk_" + f] = np.asarray(getattr(ep, f))
+        etks.append(retk.ETKParams(n_atoms=ep.n_atoms, **{f: getattr(ep, f) for f in ETK_FIELDS}))
     b = rsb.pack_shared_dg_batch(params, SYNTH_K, dim=4)
     for f in BATCH_FIELDS:
         out["sy_" + f] = np.asarray(getattr(b, f))
     out["sy_metric_seed42"] = rdg.metric_matrix_positions(b, bms, seed=42, dim=4)
     out["sy_metric_seed5_dim3"] = rdg.metric_matrix_positions(rsb.pack_shared_dg_batch(params, SYNTH_K, dim=3),
                                                               bms, seed=5, dim=3)
+    b3 = rsb.pack_shared_dg_batch(params, SYNTH_K, dim=3)
+    rsb.add_etk_to_batch(b3, etks)
+    for f in ETK_BATCH:
+        out["sy3_" + f] = np.asarray(getattr(b3, f))
     np.savez_compressed(os.path.join(HERE, "ref_dg_batches.npz"), **out)
     print("wrote", os.path.join(HERE, "ref_dg_batches.npz"), "arrays:", len(out))
 

@@ -58,6 +58,7 @@ def dg_golden_mol(g, mi: int) -> synth.SynthMol:
     bonds = [(int(i), int(j), float(o)) for i, j, o in g[pre + "bonds"]]
     mol = synth.SynthMol(list(g[pre + "elements"]), bonds, g[pre + "aromatic"].astype(bool),
                          g[pre + "ring_of"].tolist(), name=f"dg-golden-{mi}")
+    synth.assign_types(mol)
     mol.AddConformer(g[pre + "pos"])
     mol.chiral_tags = {int(c): str(t) for c, t in zip(g[pre + "chiral_centers"], g[pre + "chiral_tags"])}
     return mol
