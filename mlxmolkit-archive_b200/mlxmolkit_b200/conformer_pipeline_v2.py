@@ -1,11 +1,24 @@
-"""``generate_conformers_nk(run_mmff=True)`` with the MMFF stage on B200.
+"""``generate_conformers_nk``: distance geometry, ETK and MMFF on B200.
 
 Signature and result types of mlxmolkit/conformer_pipeline_v2.py:41-56,
-357-372.  The distance-geometry / ETK embedding stages of the reference
-(:172-290) are outside this package: molecules are embedded on the host --
-with RDKit's ETKDG for SMILES input, or taken as given for molecules that
-already carry conformers (RDKit ``Mol`` or ``SynthMol``) -- and the MMFF stage
-runs on the GPU:
+357-372, plus one additive keyword, ``embed``.
+
+Embedding (``embed="auto"`` picks per molecule):
+* ``"device"`` -- the reference's stages (:172-290) on the GPU, for ``synth``
+  molecules: DG terms from the molecule's bounds (``dg_extract.synth_dg_params``,
+  the synthetic stand-in for RDKit's bounds matrix), metric-matrix starts (seed
+  42), the 4-D DG minimisation with the budget max(300, 300 + 20 * complexity),
+  a second pass at twice the budget for the conformers that did not converge
+  when some but not all failed (improved results kept), the 4-D -> 3-D collapse
+  (200 iterations, weights 1.0 / 0.2), the 1-2 / 1-3 ETK bounds re-centred on the
+  3-D distances (:224-258: a molecule's terms take its last conformer's
+  distances, as there), then ETK (budget max(150, 150 + 10 * complexity)) unless
+  ``variant == "DG"``.  The stereo checks of :197-209 are not run (see
+  ``converged``: DG failures are reported unconverged);
+* ``"host"`` -- RDKit's ETKDG for SMILES input; molecules that carry conformers
+  (RDKit ``Mol`` or ``SynthMol``) are taken as given.
+
+MMFF stage (``run_mmff``), on the GPU:
 
 * parameters are extracted once per molecule from its first conformer
   (:299-317);
@@ -49,6 +62,7 @@ class PipelineResult:
 
 
 def _auto_iters(max_atoms: int, base: int = 200, scale: float = 15.0) -> int:
+    """The reference's iteration budgets (conformer_pipeline_v2.py:123-126)."""
     return max(base, int(base + scale * max_atoms))
 
 
@@ -72,6 +86,76 @@ def _embed(item, k: int, seed: int):
     return item, xyz[:k] if k else xyz
 
 
+def _recenter_bounds(b3, pos3: np.ndarray) -> None:
+    """Re-centre each molecule's 1-2 / 1-3 ETK bounds on the measured 3-D distances, keeping
+    their half-widths (conformer_pipeline_v2.py:224-258; the last conformer of a molecule wins)."""
+    last = {}
+    for c in range(b3.n_confs_total):
+        last[int(b3.conf_to_mol[c])] = c
+    for tag in ("12", "13"):
+        st = getattr(b3, f"etk_dist{tag}_term_starts")
+        i1, i2 = getattr(b3, f"etk_dist{tag}_idx1"), getattr(b3, f"etk_dist{tag}_idx2")
+        lb, ub = getattr(b3, f"etk_dist{tag}_lb"), getattr(b3, f"etk_dist{tag}_ub")
+        for m, c in last.items():
+            t0, t1 = int(st[m]), int(st[m + 1])
+            if t1 == t0:
+                continue
+            n = int(b3.mol_n_atoms[m])
+            a0 = int(b3.conf_atom_starts[c]) * 3
+            x = pos3[a0:a0 + 3 * n].reshape(n, 3).astype(np.float64)
+            d = np.linalg.norm(x[i1[t0:t1]] - x[i2[t0:t1]], axis=1)
+            hw = (ub[t0:t1].astype(np.float64) - lb[t0:t1]) / 2.0
+            lb[t0:t1] = (d - hw).astype(np.float32)
+            ub[t0:t1] = (d + hw).astype(np.float32)
+
+
+def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight, chiral_weight, variant,
+                     seed: int = 42):
+    """DG -> collapse -> (ETK) on the GPU; returns per molecule a list of (N, 3) conformers, whether
+    each conformer's DG and ETK stages converged, and its DG + ETK energy (:333-341)."""
+    from .conformer_metal import dg_minimize_shared
+    from .dg_extract import metric_matrix_positions, synth_dg_params
+    from .etk_extract import synth_etk_params
+    from .etk_metal import etk_minimize_shared
+    from .shared_batch import add_etk_to_batch, pack_shared_dg_batch
+    dgp = [synth_dg_params(m) for m in mols]
+    b4 = pack_shared_dg_batch(dgp, ks, dim=4)
+    C = b4.n_confs_total
+    max_atoms = max(p.n_atoms for p in dgp)
+    complexity = max(max_atoms, int(max(len(p.dist_idx1) for p in dgp) ** 0.5))
+    dg_iters = dg_max_iters if dg_max_iters > 0 else _auto_iters(complexity, 300, 20.0)
+    etk_iters = etk_max_iters if etk_max_iters > 0 else _auto_iters(complexity, 150, 10.0)
+    x4 = metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=4)
+    out4, e4, s4 = dg_minimize_shared(b4, x4, max_iters=dg_iters, fourth_dim_weight=fourth_dim_weight,
+                                      chiral_weight=chiral_weight)
+    n_failed = int(np.sum(s4 != 0))
+    if 0 < n_failed < C:                                         # :186-200
+        out2, e2, s2 = dg_minimize_shared(b4, out4, max_iters=2 * dg_iters, fourth_dim_weight=fourth_dim_weight,
+                                          chiral_weight=chiral_weight)
+        for c in np.nonzero(s4 != 0)[0]:
+            if s2[c] == 0 or e2[c] < e4[c]:
+                a0, a1 = int(b4.conf_atom_starts[c]) * 4, int(b4.conf_atom_starts[c + 1]) * 4
+                out4[a0:a1] = out2[a0:a1]
+                e4[c], s4[c] = e2[c], s2[c]
+    col, _, _ = dg_minimize_shared(b4, out4, max_iters=200, fourth_dim_weight=1.0, chiral_weight=0.2)
+    pos3 = col.reshape(-1, 4)[:, :3].reshape(-1).copy()
+    e3, s3 = np.zeros(C, np.float32), np.zeros(C, np.int32)
+    if variant != "DG":
+        b3 = pack_shared_dg_batch(dgp, ks, dim=3)
+        add_etk_to_batch(b3, [synth_etk_params(m, p.bounds_mat) for m, p in zip(mols, dgp)])
+        _recenter_bounds(b3, pos3)
+        pos3, e3, s3 = etk_minimize_shared(b3, pos3, max_iters=etk_iters)
+    confs, ok, energy, c = [], [], [], 0
+    for m, k in zip(mols, ks):
+        n = m.GetNumAtoms()
+        confs.append([pos3[(int(b4.conf_atom_starts[c + j])) * 3:(int(b4.conf_atom_starts[c + j]) + n) * 3]
+                      .reshape(n, 3).astype(np.float64) for j in range(k)])
+        ok.append([bool(s4[c + j] == 0 and s3[c + j] == 0) for j in range(k)])
+        energy.append([float(e4[c + j]) + float(e3[c + j]) for j in range(k)])
+        c += k
+    return confs, ok, energy
+
+
 def generate_conformers_nk(
     smiles_list: Sequence,
     n_confs_per_mol=10,
@@ -87,15 +171,35 @@ def generate_conformers_nk(
     mmff_max_iters: int = 0,
     mmff_use_lbfgs: Optional[bool] = None,
     mmff_variant: str = "MMFF94",
+    embed: str = "auto",
 ) -> PipelineResult:
-    """N molecules x k conformers; MMFF94/94s refinement on the GPU when ``run_mmff``."""
+    """N molecules x k conformers: embedding (DG + ETK on the GPU for ``synth`` molecules) and
+    MMFF94/94s refinement on the GPU when ``run_mmff``."""
+    if embed not in ("auto", "device", "host"):
+        raise ValueError("embed must be 'auto', 'device' or 'host'")
     t0 = time.time()
     N = len(smiles_list)
     ks = [n_confs_per_mol] * N if isinstance(n_confs_per_mol, int) else list(n_confs_per_mol)
-    embedded = [_embed(item, int(k), 42 + i) for i, (item, k) in enumerate(zip(smiles_list, ks))]
+    on_device = [embed == "device" or (embed == "auto" and hasattr(item, "distance_matrix")) for item in smiles_list]
+    embedded = [None] * N
+    dg_ok = [None] * N
+    dg_e = [None] * N
+    dev_idx = [i for i in range(N) if on_device[i]]
+    if dev_idx:
+        confs, ok, en = _embed_on_device([smiles_list[i] for i in dev_idx], [int(ks[i]) for i in dev_idx],
+                                         dg_max_iters=dg_max_iters, etk_max_iters=etk_max_iters,
+                                         fourth_dim_weight=fourth_dim_weight, chiral_weight=chiral_weight,
+                                         variant=variant)
+        for j, i in enumerate(dev_idx):
+            embedded[i] = (smiles_list[i], confs[j])
+            dg_ok[i], dg_e[i] = ok[j], en[j]
+    for i in range(N):
+        if embedded[i] is None:
+            embedded[i] = _embed(smiles_list[i], int(ks[i]), 42 + i)
     results = [ConformerResult(n_atoms=m.GetNumAtoms(), positions_3d=[x.copy() for x in xs],
-                               energies=[0.0] * len(xs), converged=[True] * len(xs))
-               for m, xs in embedded]
+                               energies=list(dg_e[i]) if dg_e[i] else [0.0] * len(xs),
+                               converged=list(dg_ok[i]) if dg_ok[i] else [True] * len(xs))
+               for i, (m, xs) in enumerate(embedded)]
     n_batches = 0
     if run_mmff and N:
         params, ok = [], []
@@ -135,7 +239,10 @@ def generate_conformers_nk(
                     xyz = r.positions[start: start + 3 * n * k].reshape(k, n, 3).astype(np.float64)
                     results[i].positions_3d = [xyz[c] for c in range(k)]
                     results[i].energies = [float(v) for v in r.energies[cursor: cursor + k]]
-                    results[i].converged = [bool(v) for v in r.converged[cursor: cursor + k]]
+                    conv = [bool(v) for v in r.converged[cursor: cursor + k]]
+                    if dg_ok[i] is not None:                  # an embedding failure stays a failure
+                        conv = [a and b for a, b in zip(conv, dg_ok[i])]
+                    results[i].converged = conv
                     cursor += k
     return PipelineResult(molecules=results, total_conformers=sum(len(r.positions_3d) for r in results),
                           total_time=time.time() - t0, n_batches=max(n_batches, 1))

@@ -135,9 +135,33 @@ def test_generate_conformers_nk_runs_the_mmff_stage():
     mols = synth.make_molecules(3, 3, 73, 8, 20, workers=1)
     bad = mols[0].copy()
     bad.types[0] = "XX"                               # untypable: marked unconverged, batch goes on
-    res = generate_conformers_nk(mols + [bad], 3, run_mmff=True, mmff_max_iters=500)
+    res = generate_conformers_nk(mols + [bad], 3, run_mmff=True, mmff_max_iters=500, embed="host")
     assert res.total_conformers == 12
     for r, m in zip(res.molecules[:3], mols):
         assert all(r.converged) and np.isfinite(r.energies).all()
         assert not np.allclose(r.positions_3d[0], m.GetConformers()[0].pos)
     assert not any(res.molecules[3].converged)
+
+
+def test_generate_conformers_nk_embeds_on_the_device():
+    """DG -> collapse -> ETK -> MMFF, all on the GPU: distinct conformers with sane geometry, the
+    reference's convergence rule (every stage converged, conformer_pipeline_v2.py:337-341)."""
+    from mlxmolkit_b200.conformer_pipeline_v2 import generate_conformers_nk
+    mols = synth.make_molecules(4, 1, 79, 8, 22, workers=1)
+    res = generate_conformers_nk(mols, 5, run_mmff=True)
+    assert res.total_conformers == 20
+    conv = np.concatenate([r.converged for r in res.molecules])
+    assert conv.mean() >= 0.75
+    for r, m in zip(res.molecules, mols):
+        assert len(r.positions_3d) == 5 and np.isfinite(r.energies).all()
+        x = np.stack(r.positions_3d)
+        assert np.abs(x[0] - x[1]).max() > 0.05                      # independent conformers
+        for b in m.GetBonds():                                       # MMFF bond lengths, not the generator's
+            i, j = b.GetBeginAtomIdx(), b.GetEndAtomIdx()
+            d = np.linalg.norm(x[:, i] - x[:, j], axis=1)
+            assert np.all((d > 0.9) & (d < 2.0)) and np.ptp(d) < 0.05, (i, j, d)
+    # embedding alone: DG + ETK energies, no MMFF
+    res0 = generate_conformers_nk(mols, 5, run_mmff=False)
+    e0 = np.concatenate([r.energies for r in res0.molecules])
+    e1 = np.concatenate([r.energies for r in res.molecules])
+    assert np.isfinite(e0).all() and not np.allclose(e0, e1)
