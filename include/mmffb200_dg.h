@@ -105,6 +105,14 @@ int mmffb_dg_minimize(const MMFFDGBatchDev *batch, const MMFFDGParams *params, f
 int mmffb_dg_energy_grad(const MMFFDGBatchDev *batch, const MMFFDGParams *params, const float *pos,
                          float *energies, float *grad, mmffb_stream_t stream);
 
+/* Stereo checks after DG (mlxmolkit/stereo_checks_metal.py:30-141): conformer c passes when every
+ * tetrahedral quad of its molecule (tet_quads[4*t..], rows tet_starts[m]..tet_starts[m+1]:
+ * neighbours n0, n1, n2 and n3 or the centre) has |V| >= vol_tol and every chiral term of the
+ * batch's DG terms has V inside [lower, upper]; V = (p0-p3).((p1-p3)x(p2-p3)) on the first
+ * three coordinates.  passed int32[n_conf] gets 1 or 0. */
+int mmffb_stereo_check(const MMFFDGBatchDev *batch, const int32_t *tet_starts, const int32_t *tet_quads,
+                       float vol_tol, const float *pos, int32_t *passed, mmffb_stream_t stream);
+
 /* The ETK stage: scratch, minimisation in place (params: max_iters, lbfgs_m, threads, grad_tol;
  * the weights are not used), and energy + gradient.  confs->dim must be 3. */
 size_t mmffb_etk_scratch_bytes(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *terms, const MMFFDGParams *params);

@@ -682,6 +682,47 @@ __global__ void __launch_bounds__(NT) energy_grad_kernel(const __grid_constant__
     if (threadIdx.x == 0) a.energy[c] = e;
 }
 
+// ---------------------------------------------------------------- stereo checks
+
+struct StereoArgs {
+    MMFFDGBatchDev b;
+    const int32_t *tet_starts, *tet_quads;
+    float vol_tol;
+    const float *pos;
+    int32_t *passed;
+};
+
+__device__ __forceinline__ float3 atom3(const float *P, int i, int dim) {
+    return make_float3(P[dim * i], P[dim * i + 1], P[dim * i + 2]);
+}
+
+__device__ __forceinline__ float quad_volume(const float *P, int dim, int4 q) {
+    const float3 p3 = atom3(P, q.w, dim);
+    const float3 v1 = sub3(atom3(P, q.x, dim), p3), v2 = sub3(atom3(P, q.y, dim), p3), v3 = sub3(atom3(P, q.z, dim), p3);
+    return dot3(v1, cross3(v2, v3));
+}
+
+// one warp per conformer
+__global__ void __launch_bounds__(128) stereo_kernel(const __grid_constant__ StereoArgs a) {
+    const int c = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (c >= a.b.n_conf) return;
+    const int mol = a.b.conf_to_mol[c], dim = a.b.dim;
+    const float *P = a.pos + (size_t)a.b.conf_atom_starts[c] * dim;
+    bool ok = true;
+    const int4 *tq = reinterpret_cast<const int4 *>(a.tet_quads);
+    for (int t = a.tet_starts[mol] + lane; t < a.tet_starts[mol + 1]; t += 32)
+        if (fabsf(quad_volume(P, dim, __ldg(tq + t))) < a.vol_tol) ok = false;
+    const int4 *cq = reinterpret_cast<const int4 *>(a.b.chiral_quads);
+    const float2 *cb = reinterpret_cast<const float2 *>(a.b.chiral_bounds);
+    for (int t = a.b.chiral_starts[mol] + lane; t < a.b.chiral_starts[mol + 1]; t += 32) {
+        const float v = quad_volume(P, dim, __ldg(cq + t));
+        const float2 bd = __ldg(cb + t);
+        if (v < bd.x || v > bd.y) ok = false;
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) a.passed[c] = ok ? 1 : 0;
+}
+
 int pick_threads(int max_atoms, int req) {
     if (req) return req;
     return max_atoms <= 48 ? 32 : max_atoms <= 96 ? 64 : max_atoms <= 192 ? 128 : 256;
@@ -921,6 +962,20 @@ int mmffb_etk_energy_grad(const MMFFDGBatchDev *confs, const MMFFETKTermsDev *te
     int r = check_etk(confs, terms, params);
     if (r) return r;
     return energy_grad(confs, terms, params, kETK, pos, energies, grad, stream);
+}
+
+int mmffb_stereo_check(const MMFFDGBatchDev *batch, const int32_t *tet_starts, const int32_t *tet_quads,
+                       float vol_tol, const float *pos, int32_t *passed, mmffb_stream_t stream) {
+    if (!batch) return fail(MMFFB_EINVAL, "null batch");
+    if (batch->n_conf < 0 || (batch->dim != 3 && batch->dim != 4)) return fail(MMFFB_EINVAL, "bad conformer count or dim");
+    if (batch->n_conf == 0) return 0;
+    if (!batch->conf_to_mol || !batch->conf_atom_starts || !batch->chiral_starts || !tet_starts || !pos || !passed)
+        return fail(MMFFB_EINVAL, "null pointer");
+    StereoArgs a{*batch, tet_starts, tet_quads, vol_tol, pos, passed};
+    stereo_kernel<<<(batch->n_conf + 3) / 4, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "stereo_kernel launch");
+    return 0;
 }
 
 }  // extern "C"

@@ -84,7 +84,7 @@ EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_mini
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
            "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step",
            "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad",
-           "mmffb_etk_scratch_bytes", "mmffb_etk_minimize", "mmffb_etk_energy_grad"]
+           "mmffb_etk_scratch_bytes", "mmffb_etk_minimize", "mmffb_etk_energy_grad", "mmffb_stereo_check"]
 
 _lib = None
 
@@ -138,6 +138,8 @@ def load():
     L.mmffb_etk_minimize.argtypes = [DBP, ETP, DPP, P, P, P, P, P, ctypes.c_size_t, P]
     L.mmffb_etk_energy_grad.restype = ctypes.c_int
     L.mmffb_etk_energy_grad.argtypes = [DBP, ETP, DPP, P, P, P, P]
+    L.mmffb_stereo_check.restype = ctypes.c_int
+    L.mmffb_stereo_check.argtypes = [DBP, P, P, ctypes.c_float, P, P, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int
     L.mmffb_minimize_noalloc.argtypes = [BP, CP, OP, P, P, P, P, P, P]
     _lib = L

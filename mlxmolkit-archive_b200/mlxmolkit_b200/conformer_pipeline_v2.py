@@ -13,8 +13,9 @@ Embedding (``embed="auto"`` picks per molecule):
   (200 iterations, weights 1.0 / 0.2), the 1-2 / 1-3 ETK bounds re-centred on the
   3-D distances (:224-258: a molecule's terms take its last conformer's
   distances, as there), then ETK (budget max(150, 150 + 10 * complexity)) unless
-  ``variant == "DG"``.  The stereo checks of :197-209 are not run (see
-  ``converged``: DG failures are reported unconverged);
+  ``variant == "DG"``.  The stereo checks of :197-209 run on the GPU after the
+  DG passes (``stereo_checks.run_stereo_checks``); a conformer that fails them
+  is reported unconverged;
 * ``"host"`` -- RDKit's ETKDG for SMILES input; molecules that carry conformers
   (RDKit ``Mol`` or ``SynthMol``) are taken as given.
 
@@ -137,6 +138,9 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
                 a0, a1 = int(b4.conf_atom_starts[c]) * 4, int(b4.conf_atom_starts[c + 1]) * 4
                 out4[a0:a1] = out2[a0:a1]
                 e4[c], s4[c] = e2[c], s2[c]
+    from .stereo_checks import run_stereo_checks                   # :197-209: a failure is DG status 2
+    passed = run_stereo_checks(out4, dgp, mols, b4.conf_atom_starts, b4.conf_to_mol, list(range(len(mols))), C, dim=4)
+    s4 = np.where(passed, s4, 2).astype(np.int32)
     col, _, _ = dg_minimize_shared(b4, out4, max_iters=200, fourth_dim_weight=1.0, chiral_weight=0.2)
     pos3 = col.reshape(-1, 4)[:, :3].reshape(-1).copy()
     e3, s3 = np.zeros(C, np.float32), np.zeros(C, np.int32)

@@ -28,6 +28,7 @@ def install():
     chem.AssignStereochemistry = lambda mol, cleanIt=True, force=True: None
     synth.SynthAtom.GetChiralTag = lambda atom: _ChiralType.BY_NAME.get(
         (getattr(atom._mol, "chiral_tags", None) or {}).get(atom.GetIdx()), _ChiralType.CHI_UNSPECIFIED)
+    synth.SynthMol.GetRingInfo = lambda mol: _RingInfo(mol)
     dg = types.ModuleType("rdkit.Chem.rdDistGeom")
     chem.rdDistGeom = dg
     rdkit.Chem = chem
@@ -52,3 +53,17 @@ def import_reference(ref_root: str):
     params = importlib.import_module("mlxmolkit.mmff_params")
     vec = importlib.import_module("mlxmolkit.mmff_energy_vectorized")
     return params, vec
+
+
+class _RingInfo:
+    """RingInfo over a SynthMol's ring ids (``ring_of``: one ring per atom, -1 outside rings)."""
+
+    def __init__(self, mol):
+        self.ring_of = list(mol.ring_of)
+
+    def NumAtomRings(self, idx):
+        return 1 if self.ring_of[idx] >= 0 else 0
+
+    def IsAtomInRingOfSize(self, idx, size):
+        r = self.ring_of[idx]
+        return r >= 0 and sum(1 for x in self.ring_of if x == r) == size

@@ -14,7 +14,10 @@ the REFERENCE's own mlxmolkit/dg_extract.py (``extract_dg_params``,
   * seeded synthetic molecules whose bounds matrix and chiral tags come from
     this package's stand-ins (``synth_bounds_matrix``, ``synth_chiral_tags``),
     and their ETK terms (``etk_extract.synth_etk_params``) through the
-    reference's ``add_etk_to_batch`` (mlxmolkit/shared_batch.py:204-296),
+    reference's ``add_etk_to_batch`` (mlxmolkit/shared_batch.py:204-296), and the
+    reference's stereo checks (mlxmolkit/stereo_checks_metal.py:102-141,
+    ``extract_tetrahedral_data``) on their conformers as embedded, mirrored and
+    flattened,
 
 and stores the inputs and the reference's outputs in
 ``tests/golden/ref_dg_batches.npz``.  The tests compare this package's
@@ -75,6 +78,7 @@ def main(ref_root: str) -> None:
     rdg = importlib.import_module("mlxmolkit.dg_extract")
     rsb = importlib.import_module("mlxmolkit.shared_batch")
     retk = importlib.import_module("mlxmolkit.etk_extract")
+    rst = importlib.import_module("mlxmolkit.stereo_checks_metal")
     out = {}
 
     # all-pairs sets of the reference's tests
@@ -85,7 +89,7 @@ def main(ref_root: str) -> None:
     out["ap_init_seed7"] = rsb.init_random_positions(b, seed=7)
 
     # synthetic molecules through the reference's extraction
-    params, bms, etks = [], [], []
+    params, bms, etks, mols = [], [], [], []
     for mi, (seed, lo, hi) in enumerate(SYNTH):
         rng = np.random.default_rng(seed)
         mol = synth.generate_molecule(rng, lo, hi, name=f"dg-golden-{mi}")
@@ -107,6 +111,9 @@ def main(ref_root: str) -> None:
             out[pre + "ref_" + f] = np.asarray(getattr(p, f))
         params.append(p)
         bms.append(bm)
+        mols.append(mol)
+        tet = rdg.extract_tetrahedral_data(mol)
+        out[pre + "ref_tetrahedral"] = np.array(tet[:5], dtype=np.int32).reshape(5, -1)
         ep = synth_etk_params(mol, bm)
         for f in ETK_FIELDS:
             out[pre + "etk_" + f] = np.asarray(getattr(ep, f))
@@ -117,6 +124,24 @@ def main(ref_root: str) -> None:
     out["sy_metric_seed42"] = rdg.metric_matrix_positions(b, bms, seed=42, dim=4)
     out["sy_metric_seed5_dim3"] = rdg.metric_matrix_positions(rsb.pack_shared_dg_batch(params, SYNTH_K, dim=3),
                                                               bms, seed=5, dim=3)
+    # stereo checks: conformer j of a molecule as embedded (j = 0), mirrored (1: chirality inverted),
+    # flattened onto z = 0 (2: planar centres)
+    pos4 = np.zeros((int(b.conf_atom_starts[-1]), 4), np.float32)
+    c = 0
+    for mol, k in zip(mols, SYNTH_K):
+        x = np.asarray(mol.GetConformers()[0].pos, dtype=np.float32)
+        for j in range(k):
+            y = x.copy()
+            if j == 1:
+                y[:, 0] = -y[:, 0]
+            elif j == 2:
+                y[:, 2] = 0.0
+            a0 = int(b.conf_atom_starts[c])
+            pos4[a0:a0 + len(x), :3] = y
+            c += 1
+    out["sy_stereo_pos4"] = pos4.reshape(-1)
+    out["sy_stereo_passed"] = rst.run_stereo_checks(pos4.reshape(-1), params, mols, b.conf_atom_starts,
+                                                    b.conf_to_mol, list(range(len(mols))), b.n_confs_total, dim=4)
     b3 = rsb.pack_shared_dg_batch(params, SYNTH_K, dim=3)
     rsb.add_etk_to_batch(b3, etks)
     for f in ETK_BATCH:

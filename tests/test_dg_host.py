@@ -194,3 +194,14 @@ def test_device_layout_rejects_bad_indices():
         dg_device_arrays(pack_shared_dg_batch([p], [1]))
     with pytest.raises(ValueError):
         dg_device_arrays(pack_shared_dg_batch([all_pairs_dg(4)], [1], dim=5))
+
+
+def test_tetrahedral_centres_match_the_reference(dg_golden):
+    from mlxmolkit_b200.stereo_checks import extract_tetrahedral_data, tetrahedral_quads
+    for mi in range(3):
+        mol = dg_golden_mol(dg_golden, mi)
+        ref = dg_golden[f"s{mi}_ref_tetrahedral"]
+        got = np.array(extract_tetrahedral_data(mol)[:5], dtype=np.int32).reshape(5, -1)
+        assert np.array_equal(got, ref), mi
+        q = tetrahedral_quads(mol)
+        assert np.array_equal(q, ref[1:5].T)

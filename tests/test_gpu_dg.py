@@ -111,3 +111,20 @@ def test_runs_are_bit_identical_and_thread_counts_agree():
         r = dg_minimize_shared(b, x0, max_iters=5, tpm=tpm)
         np.testing.assert_allclose(r[1], ref[1], rtol=1e-3, atol=1e-3)
         assert np.array_equal(r[2], ref[2])
+
+
+def test_stereo_checks_match_the_reference(dg_golden):
+    """The reference's own run_stereo_checks verdicts (stereo_checks_metal.py:102-141) on conformers
+    as embedded, mirrored and flattened (tests/golden/ref_dg_batches.npz)."""
+    from helpers import dg_golden_mol
+    from mlxmolkit_b200.stereo_checks import run_stereo_checks
+    fields = ("dist_idx1", "dist_idx2", "dist_lb2", "dist_ub2", "dist_weight", "chiral_idx1", "chiral_idx2",
+              "chiral_idx3", "chiral_idx4", "chiral_vol_lower", "chiral_vol_upper", "fourth_idx")
+    params = [DGParams(n_atoms=len(dg_golden[f"s{mi}_elements"]), **{f: dg_golden[f"s{mi}_ref_{f}"] for f in fields})
+              for mi in range(3)]
+    mols = [dg_golden_mol(dg_golden, mi) for mi in range(3)]
+    b = pack_shared_dg_batch(params, [2, 3, 1], dim=4)
+    got = run_stereo_checks(dg_golden["sy_stereo_pos4"], params, mols, b.conf_atom_starts, b.conf_to_mol,
+                            [0, 1, 2], b.n_confs_total, dim=4)
+    ref = dg_golden["sy_stereo_passed"]
+    assert np.array_equal(got, ref) and (~ref).any() and ref.any()
