@@ -209,6 +209,7 @@ typedef struct {
     float max_step_per_atom;
     float grad_tol;         /* largest per-atom norm of the scaled gradient */
     double mode[4];         /* term constants, as MMFFOptParams.mode */
+    int32_t threads;        /* threads per conformer: 64, 128 or 256; 0 = chosen from the batch */
 } MMFFMultiMolParams;
 
 enum {

@@ -19,7 +19,6 @@
 namespace mmffb {
 namespace {
 
-constexpr int kMMThreads = 256;
 constexpr double kEpsCurv = 1e-10;   // mmff_metal_optimizer.py:31
 
 struct MMArgs {
@@ -31,14 +30,16 @@ struct MMArgs {
     int nv;                    // history row stride
 };
 
+template <int NW>
 __device__ __forceinline__ double block_sum(double v, double *red) {
     double s[1] = {v}, z[1] = {0.0};
-    block_reduce<kMMThreads / 32, 1, 1, double>(s, z, red);
+    block_reduce<NW, 1, 1, double>(s, z, red);
     return s[0];
 }
 
-__global__ void __launch_bounds__(kMMThreads) multimol_kernel(const MMArgs a) {
-    constexpr int NT = kMMThreads, NW = NT / 32;
+template <int NT>
+__global__ void __launch_bounds__(NT) multimol_kernel(const MMArgs a) {
+    constexpr int NW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     const Params &P = a.P;
     Layout L = make_layout(P.nmax, NW, 1, true, sizeof(float), sizeof(double), P.b.max_classes);
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(kMMThreads) multimol_kernel(const MMArgs a) {
             for (int w = 0; w < NW; ++w) s += gbuf[(size_t)w * nv + k];
             gv[k] = s * a.grad_scale;
         }
-        e = block_sum(ep, red());
+        e = block_sum<NW>(ep, red());
     };
 
     double e = 0.0;
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(kMMThreads) multimol_kernel(const MMArgs a) {
             const float *s_i = Sh + (size_t)sl * a.nv, *y_i = Yh + (size_t)sl * a.nv;
             double t = 0.0;
             for (int k = tid; k < n; k += NT) t += (double)s_i[k] * qv[k];
-            const double ai = (double)rho[sl] * block_sum(t, red());
+            const double ai = (double)rho[sl] * block_sum<NW>(t, red());
             if (tid == 0) alpha[i] = ai;
             const float af = (float)ai;
             for (int k = tid; k < n; k += NT) qv[k] -= af * y_i[k];
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kMMThreads) multimol_kernel(const MMArgs a) {
             const float *s_i = Sh + (size_t)sl * a.nv, *y_i = Yh + (size_t)sl * a.nv;
             double t = 0.0;
             for (int k = tid; k < n; k += NT) t += (double)y_i[k] * qv[k];
-            const double beta = (double)rho[sl] * block_sum(t, red());
+            const double beta = (double)rho[sl] * block_sum<NW>(t, red());
             const float c = (float)(alpha[i] - beta);
             for (int k = tid; k < n; k += NT) qv[k] += s_i[k] * c;
             __syncthreads();
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(kMMThreads) multimol_kernel(const MMArgs a) {
             y_n[k] = y;
             t += (double)dv[k] * y;
         }
-        const double sy = block_sum(t, red());
+        const double sy = block_sum<NW>(t, red());
         if (tid == 0) rho[sl] = sy > kEpsCurv ? (float)(1.0 / (sy + 1e-30)) : 0.f;
         ++hcount;
         __threadfence_block();
@@ -263,18 +264,41 @@ extern "C" int mmffb_multimol_step(const MMFFBatchDev *batch, const MMFFConfDev 
     a.it_end = it_end;
     a.max_iters = max_iters;
     a.nv = (3 * confs->max_atoms + 3) & ~3;
-    const Layout L = make_layout(confs->max_atoms, kMMThreads / 32, 1, true, sizeof(float), sizeof(double),
-                                 batch->max_classes);
-    int dev = 0, optin = 0;
+    if (prm->threads != 0 && prm->threads != 64 && prm->threads != 128 && prm->threads != 256)
+        return fail(MMFFB_EINVAL, "threads must be 0, 64, 128 or 256");
+    int dev = 0, optin = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(smem)");
-    if (L.total > (size_t)optin)
-        return fail(MMFFB_ETOOBIG, "molecule of %d atoms needs %zu B of shared memory", confs->max_atoms, L.total);
-    e = cudaFuncSetAttribute(multimol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-    multimol_kernel<<<confs->n_conf, kMMThreads, L.total, reinterpret_cast<cudaStream_t>(stream)>>>(a);
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+    // Threads per conformer: as given, else the largest instance whose resident CTAs hold every
+    // conformer (one wave per launch), else 64 (the most CTAs per wave).
+    int nt = prm->threads;
+    size_t smem = 0;
+    for (int cand = prm->threads ? prm->threads : 256; cand >= 64; cand /= 2) {
+        const Layout L = make_layout(confs->max_atoms, cand / 32, 1, true, sizeof(float), sizeof(double),
+                                     batch->max_classes);
+        if (L.total > (size_t)optin) continue;
+        const void *fn = cand == 256 ? (const void *)&multimol_kernel<256>
+                         : cand == 128 ? (const void *)&multimol_kernel<128> : (const void *)&multimol_kernel<64>;
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+        int occ = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, cand, L.total);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        nt = cand;
+        smem = L.total;
+        if (prm->threads || (long long)sms * occ >= confs->n_conf) break;
+    }
+    if (smem == 0)
+        return fail(MMFFB_ETOOBIG, "molecule of %d atoms does not fit the multimol kernel's shared memory",
+                    confs->max_atoms);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (nt == 256) multimol_kernel<256><<<confs->n_conf, 256, smem, st>>>(a);
+    else if (nt == 128) multimol_kernel<128><<<confs->n_conf, 128, smem, st>>>(a);
+    else multimol_kernel<64><<<confs->n_conf, 64, smem, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "multimol_kernel launch");
     return 0;

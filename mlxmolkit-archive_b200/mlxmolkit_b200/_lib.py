@@ -50,7 +50,7 @@ class MMFFMultiMolState(ctypes.Structure):
 class MMFFMultiMolParams(ctypes.Structure):
     _fields_ = [("history_m", ctypes.c_int32), ("grad_scale", ctypes.c_float),
                 ("max_step_per_atom", ctypes.c_float), ("grad_tol", ctypes.c_float),
-                ("mode", ctypes.c_double * 4)]
+                ("mode", ctypes.c_double * 4), ("threads", ctypes.c_int32)]
 
 
 MM_START, MM_REVERT, MM_RUN, MM_MAIN_CHECK, MM_POLISH_CHECK = 0, 1, 2, 3, 4

@@ -93,7 +93,7 @@ class _MultiMolRun:
     """Device state of one multi-molecule L-BFGS run (the reference's loop variables)."""
 
     def __init__(self, m: mm.Minimizer, pos: np.ndarray, lbfgs_m: int, grad_scale: float,
-                 max_step_per_atom: float, grad_tol: float, mode=mm.MODE_MEGA):
+                 max_step_per_atom: float, grad_tol: float, mode=mm.MODE_MEGA, threads: int = 0):
         import torch
         self.torch, self.m, self.L = torch, m, _lib.load()
         dev = m.batch.device
@@ -116,7 +116,7 @@ class _MultiMolRun:
             self.x, self.g, self.best_x, self.e, self.best_e, self.hist, self.rho, self.hcount,
             self.converged, self.conv_iter, self.pending)))
         self.prm = _lib.MMFFMultiMolParams(self.hist_m, float(grad_scale), float(max_step_per_atom),
-                                           float(grad_tol), (ctypes.c_double * 4)(*mode))
+                                           float(grad_tol), (ctypes.c_double * 4)(*mode), int(threads))
 
     def step(self, phase: int, n_iters: int = 0, it_end: int = 0, max_iters: int = 0) -> None:
         rc = self.L.mmffb_multimol_step(ctypes.byref(self.bd), ctypes.byref(self.cd), ctypes.byref(self.prm),
@@ -157,13 +157,17 @@ def mmff_optimize_metal_multi_mol(
     grad_scale: float = 0.1,
     grad_tol: float = 1e-4,
     mmff_variant: str = "MMFF94",
+    threads: int = 0,
 ) -> MultiMolResult:
-    """Optimise many molecules' conformers with the reference's multi-molecule L-BFGS."""
+    """Optimise many molecules' conformers with the reference's multi-molecule L-BFGS.
+
+    ``threads`` (additive) fixes the threads per conformer (64, 128 or 256); 0 chooses them
+    from the batch."""
     if eval_freq < 1:
         raise ValueError("eval_freq must be >= 1")
     mols, conf_ids, params, counts, pos = _collect(mol_specs, mmff_variant)
     m = mm.Minimizer(params, counts)
-    run = _MultiMolRun(m, pos, lbfgs_m, grad_scale, max_step_per_atom, grad_tol)
+    run = _MultiMolRun(m, pos, lbfgs_m, grad_scale, max_step_per_atom, grad_tol, threads=threads)
     iters_used = run.run(int(max_iters), int(eval_freq))
     best_x = run.best_x.cpu().numpy()
     best_e = run.best_e.cpu().numpy()

@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--iters", default="1000,2000")
     ap.add_argument("--fused-iters", default="200,500,1000,2000")
     ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--threads", default="0", help="multi-mol threads per conformer: a comma list of 0/64/128/256")
     ap.add_argument("--scale", type=float, default=1.0)
     a = ap.parse_args()
     import torch
@@ -44,8 +45,8 @@ def main():
                                                 mode=mm.MODE_MEGA)
     C = int(sum(counts))
     out = {"workload": f"small-50x50-heavy10-30 x scale {a.scale}", "conformers": C, "runs": []}
-    legs = [("multi", int(v)) for v in a.iters.split(",") if v] + \
-           [("fused", int(v)) for v in a.fused_iters.split(",") if v]
+    legs = [("multi", int(v), int(t)) for v in a.iters.split(",") if v for t in a.threads.split(",")] + \
+           [("fused", int(v), 0) for v in a.fused_iters.split(",") if v]
     def run(fn, iters):
         for m, s in zip(wl.mols, start):                  # every run starts from the same coordinates
             for c, x in zip(m.GetConformers(), s):
@@ -56,8 +57,12 @@ def main():
         torch.cuda.synchronize()
         return r, time.perf_counter() - t
 
-    for api, iters in legs:
-        fn = mmff_optimize_metal_multi_mol if api == "multi" else mmff_optimize_metal_fused_multi_mol
+    for api, iters, threads in legs:
+        if api == "multi":
+            def fn(specs, max_iters, _t=threads):
+                return mmff_optimize_metal_multi_mol(specs, max_iters=max_iters, threads=_t)
+        else:
+            fn = mmff_optimize_metal_fused_multi_mol
         run(fn, iters)                                    # untimed warm-up, as the reference's script does
         times = []
         for _ in range(a.repeats):
@@ -66,7 +71,7 @@ def main():
         dt = float(np.median(times))
         e = np.concatenate([mr.energies for mr in r.mol_results]).astype(np.float64)
         d = np.abs(e - ref.energies)
-        out["runs"].append({"api": api, "max_iters": iters, "seconds": dt, "ms_per_conformer": dt * 1e3 / C,
+        out["runs"].append({"api": api, "max_iters": iters, "threads": threads or "auto", "seconds": dt, "ms_per_conformer": dt * 1e3 / C,
                             "within_0.1_kcal": int(np.sum(d <= 0.1)), "mean_abs_dE": float(d.mean()),
                             "n_iters": int(r.mol_results[0].n_iters),
                             "converged": (int(sum(int(mr.converged.sum()) for mr in r.mol_results))
