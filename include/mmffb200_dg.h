@@ -78,6 +78,7 @@ typedef struct {
     float grad_tol;            /* gradient exit (conformer_metal.py:495-503) */
     float chiral_weight;       /* weight of every chiral term */
     float fourth_dim_weight;   /* weight of every fourth-dimension term */
+    int32_t hist_mode;         /* L-BFGS history: 0 or 2 = a device slot per CTA, 1 = shared memory */
 } MMFFDGParams;
 
 typedef struct {

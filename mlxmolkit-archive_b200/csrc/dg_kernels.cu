@@ -461,7 +461,7 @@ __device__ __forceinline__ void ff_gradient(const Args &a, const float4 *X, floa
     else etk_gradient<NT>(a, X, G, mol, N, base, TG);
 }
 
-template <int NT, int FF>
+template <int NT, int FF, bool HS>
 __global__ void __launch_bounds__(NT) lbfgs_kernel(const __grid_constant__ Args a) {
     constexpr int NW = NT / 32;
     extern __shared__ float4 sm[];
@@ -476,7 +476,8 @@ __global__ void __launch_bounds__(NT) lbfgs_kernel(const __grid_constant__ Args 
         rsel ^= 1;
         return rbase + rsel * NW * 4;
     };
-    float4 *S = a.hist + (size_t)blockIdx.x * 2 * M * NA, *Y = S + (size_t)M * NA;
+    // L-BFGS history: in shared memory after the Fourier-term rows (HS), else this CTA's device slot
+    float4 *S = HS ? TG + 4 * a.tor_slots : a.hist + (size_t)blockIdx.x * 2 * M * NA, *Y = S + (size_t)M * NA;
     const MMFFDGBatchDev &b = a.b;
     const int dim = b.dim, max_iters = a.p.max_iters;
 
@@ -730,22 +731,25 @@ int pick_threads(int max_atoms, int req) {
 
 // shared memory of a CTA: `vectors` float4 vectors of na atoms, the reduction halves, the
 // L-BFGS rho values and (ETK) four gradient rows per Fourier term
-size_t smem_bytes(int nt, int na, int vectors, int tor_slots) {
+size_t smem_bytes(int nt, int na, int vectors, int tor_slots, int hist_rows = 0) {
     return (size_t)vectors * na * sizeof(float4) + (size_t)2 * (nt / 32) * 4 * sizeof(float) +
-           kMaxHist * sizeof(float) + (size_t)4 * tor_slots * sizeof(float4);
+           kMaxHist * sizeof(float) + (size_t)4 * tor_slots * sizeof(float4) + (size_t)hist_rows * na * sizeof(float4);
 }
 
-template <int FF>
+template <int FF, bool HS>
 const void *minimize_kernel_ff(int nt) {
     switch (nt) {
-        case 32: return reinterpret_cast<const void *>(&lbfgs_kernel<32, FF>);
-        case 64: return reinterpret_cast<const void *>(&lbfgs_kernel<64, FF>);
-        case 128: return reinterpret_cast<const void *>(&lbfgs_kernel<128, FF>);
-        default: return reinterpret_cast<const void *>(&lbfgs_kernel<256, FF>);
+        case 32: return reinterpret_cast<const void *>(&lbfgs_kernel<32, FF, HS>);
+        case 64: return reinterpret_cast<const void *>(&lbfgs_kernel<64, FF, HS>);
+        case 128: return reinterpret_cast<const void *>(&lbfgs_kernel<128, FF, HS>);
+        default: return reinterpret_cast<const void *>(&lbfgs_kernel<256, FF, HS>);
     }
 }
 
-const void *minimize_kernel_for(int nt, int ff) { return ff == kDG ? minimize_kernel_ff<kDG>(nt) : minimize_kernel_ff<kETK>(nt); }
+const void *minimize_kernel_for(int nt, int ff, bool hs) {
+    if (ff == kDG) return hs ? minimize_kernel_ff<kDG, true>(nt) : minimize_kernel_ff<kDG, false>(nt);
+    return hs ? minimize_kernel_ff<kETK, true>(nt) : minimize_kernel_ff<kETK, false>(nt);
+}
 
 template <int FF>
 const void *energy_kernel_ff(int nt) {
@@ -767,6 +771,7 @@ int check_confs(const MMFFDGBatchDev *b, const MMFFDGParams *p) {
         return fail(MMFFB_ETOOBIG, "max_atoms %d outside 1..1024", b->max_atoms);
     if (p->lbfgs_m < 1 || p->lbfgs_m > kMaxHist) return fail(MMFFB_EINVAL, "lbfgs_m %d outside 1..%d", p->lbfgs_m, kMaxHist);
     if (p->max_iters < 0) return fail(MMFFB_EINVAL, "negative max_iters");
+    if (p->hist_mode < 0 || p->hist_mode > 2) return fail(MMFFB_EINVAL, "hist_mode must be 0, 1 or 2");
     if (p->threads != 0 && p->threads != 32 && p->threads != 64 && p->threads != 128 && p->threads != 256)
         return fail(MMFFB_EINVAL, "threads must be 0, 32, 64, 128 or 256");
     if (b->n_conf > 0 && (!b->conf_to_mol || !b->conf_atom_starts || !b->mol_n_atoms || !b->mol_atom_base))
@@ -794,10 +799,13 @@ int check_etk(const MMFFDGBatchDev *b, const MMFFETKTermsDev *e, const MMFFDGPar
     return 0;
 }
 
-// resident CTAs per SM of the minimise kernel with nt threads
-int occupancy(int nt, int ff, int max_atoms, int tor_slots, int *occ, size_t *smem_out) {
-    const size_t smem = smem_bytes(nt, max_atoms, 6, tor_slots);
-    const void *fn = minimize_kernel_for(nt, ff);
+// resident CTAs per SM of the minimise kernel with nt threads (0 when it does not fit)
+int occupancy(int nt, int ff, bool hs, int hist_m, int max_atoms, int tor_slots, int *occ, size_t *smem_out) {
+    const size_t smem = smem_bytes(nt, max_atoms, 6, tor_slots, hs ? 2 * hist_m : 0);
+    *occ = 0;
+    *smem_out = smem;
+    if (smem > 227 * 1024) return 0;
+    const void *fn = minimize_kernel_for(nt, ff, hs);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(L-BFGS)");
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, nt, smem);
@@ -812,39 +820,54 @@ int occupancy(int nt, int ff, int max_atoms, int tor_slots, int *occ, size_t *sm
 // per conformer pay), else the size-based default (measured on B200: 1000 conformers of
 // <= 77 atoms 8.9k / 15.6k / 18.1k / 18.9k conformers/s at 32 / 64 / 128 / 256 threads;
 // 10000 conformers of <= 87 atoms 55k / 70k / 52k / 37k).
+//
+// History placement: a device slot per CTA unless hist_mode = 1 asks for shared memory.  The
+// slot is read back by the CTA that wrote it and stays in L1; in shared memory it only takes
+// L1 capacity from the term records (measured on B200, DG stage: 20 x 50 16.1k vs 18.6k and
+// 1000 x 10 54k vs 70k conformers/s, shared vs device).
 int plan_grid(const MMFFDGBatchDev *b, const MMFFDGParams *p, int ff, int tor_slots, int *nt_out, size_t *smem_out,
-              int *grid_out) {
+              int *grid_out, bool *hs_out) {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+    const int M = p->lbfgs_m;
     int nt = pick_threads(b->max_atoms, p->threads);
     size_t smem = 0;
     if (p->threads == 0)
         for (int cand = 256; cand > nt; cand /= 2) {
-            int r = occupancy(cand, ff, b->max_atoms, tor_slots, &occ, &smem);
+            int r = occupancy(cand, ff, false, M, b->max_atoms, tor_slots, &occ, &smem);
             if (r) return r;
             if (occ >= 1 && (long long)sms * occ >= b->n_conf) {
                 nt = cand;
                 break;
             }
         }
-    int r = occupancy(nt, ff, b->max_atoms, tor_slots, &occ, &smem);
+    int occ_g = 0, occ_s = 0;
+    size_t smem_g = 0, smem_s = 0;
+    int r = occupancy(nt, ff, false, M, b->max_atoms, tor_slots, &occ_g, &smem_g);
     if (r) return r;
+    r = occupancy(nt, ff, true, M, b->max_atoms, tor_slots, &occ_s, &smem_s);
+    if (r) return r;
+    const bool hs = p->hist_mode == 1;
+    if (hs && occ_s < 1) return fail(MMFFB_ETOOBIG, "the history does not fit in shared memory (%zu B)", smem_s);
+    occ = hs ? occ_s : occ_g;
+    smem = hs ? smem_s : smem_g;
     if (occ < 1) return fail(MMFFB_ETOOBIG, "the L-BFGS kernel does not fit an SM (%zu B shared memory)", smem);
     long long g = (long long)sms * occ;
     if (g > b->n_conf) g = b->n_conf;
     *nt_out = nt;
     *smem_out = smem;
     *grid_out = (int)g;
+    *hs_out = hs;
     return 0;
 }
 
 constexpr size_t kCounterBytes = 256;
 
-size_t scratch_for(const MMFFDGBatchDev *b, const MMFFDGParams *p, int grid) {
-    return kCounterBytes + (size_t)grid * 2 * p->lbfgs_m * b->max_atoms * sizeof(float4);
+size_t scratch_for(const MMFFDGBatchDev *b, const MMFFDGParams *p, int grid, bool hs) {
+    return kCounterBytes + (hs ? 0 : (size_t)grid * 2 * p->lbfgs_m * b->max_atoms * sizeof(float4));
 }
 
 int minimize(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGParams *p, int ff, float *pos,
@@ -855,9 +878,10 @@ int minimize(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGPa
     const int tor_slots = ff == kETK ? etk->max_tor : 0;
     int nt = 0, grid = 0;
     size_t smem = 0;
-    int r = plan_grid(b, p, ff, tor_slots, &nt, &smem, &grid);
+    bool hs = false;
+    int r = plan_grid(b, p, ff, tor_slots, &nt, &smem, &grid, &hs);
     if (r) return r;
-    const size_t need = scratch_for(b, p, grid);
+    const size_t need = scratch_for(b, p, grid, hs);
     if (!scratch || scratch_bytes < need)
         return fail(MMFFB_ESCRATCH, "scratch of %zu B given, %zu B needed", scratch_bytes, need);
     Args a;
@@ -877,7 +901,7 @@ int minimize(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const MMFFDGPa
     cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(L-BFGS counter)");
     void *args[] = {&a};
-    e = cudaLaunchKernel(minimize_kernel_for(nt, ff), dim3(grid), dim3(nt), args, smem, st);
+    e = cudaLaunchKernel(minimize_kernel_for(nt, ff, hs), dim3(grid), dim3(nt), args, smem, st);
     if (e != cudaSuccess) return cuda_fail(e, "lbfgs_kernel launch");
     return 0;
 }
@@ -913,8 +937,9 @@ size_t scratch_bytes(const MMFFDGBatchDev *b, const MMFFETKTermsDev *etk, const 
     if (b->n_conf == 0) return kCounterBytes;
     int nt = 0, grid = 0;
     size_t smem = 0;
-    if (plan_grid(b, p, ff, ff == kETK ? etk->max_tor : 0, &nt, &smem, &grid)) return 0;
-    return scratch_for(b, p, grid);
+    bool hs = false;
+    if (plan_grid(b, p, ff, ff == kETK ? etk->max_tor : 0, &nt, &smem, &grid, &hs)) return 0;
+    return scratch_for(b, p, grid, hs);
 }
 
 }  // namespace dg

@@ -68,7 +68,7 @@ class MMFFDGBatchDev(ctypes.Structure):
 class MMFFDGParams(ctypes.Structure):
     _fields_ = [("max_iters", ctypes.c_int32), ("lbfgs_m", ctypes.c_int32), ("threads", ctypes.c_int32),
                 ("grad_tol", ctypes.c_float), ("chiral_weight", ctypes.c_float),
-                ("fourth_dim_weight", ctypes.c_float)]
+                ("fourth_dim_weight", ctypes.c_float), ("hist_mode", ctypes.c_int32)]
 
 
 class MMFFETKTermsDev(ctypes.Structure):

@@ -64,10 +64,13 @@ class DGDeviceBatch:
 
     @staticmethod
     def params(max_iters: int, grad_tol: float, chiral_weight: float, fourth_dim_weight: float,
-               lbfgs_m: int = DEFAULT_LBFGS_M, tpm: Optional[int] = DEFAULT_TPM) -> _lib.MMFFDGParams:
+               lbfgs_m: int = DEFAULT_LBFGS_M, tpm: Optional[int] = DEFAULT_TPM,
+               hist_mode: int = 0) -> _lib.MMFFDGParams:
+        """hist_mode: where the L-BFGS history lives -- 0 or 2 a device slot per CTA (the faster,
+        measured), 1 shared memory."""
         return _lib.MMFFDGParams(max_iters=int(max_iters), lbfgs_m=int(lbfgs_m), threads=int(tpm or 0),
                                  grad_tol=float(grad_tol), chiral_weight=float(chiral_weight),
-                                 fourth_dim_weight=float(fourth_dim_weight))
+                                 fourth_dim_weight=float(fourth_dim_weight), hist_mode=int(hist_mode))
 
     def scratch(self, prm: _lib.MMFFDGParams):
         torch = _torch()

@@ -77,13 +77,13 @@ def _sub_batch(b, confs):
     return pack_shared_dg_batch(ps, counts, dim=b.dim), ordered
 
 
-def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=None) -> dict:
+def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=None, hist_mode: int = 0) -> dict:
     import torch
     b4, x0, iters, max_atoms, b3, etk_iters = _workload(n_mols, k, seed)
     C = b4.n_confs_total
     dev = DGDeviceBatch(b4)
-    p1 = dev.params(iters, 1e-4, 1.0, 0.1, tpm=tpm)
-    p2 = dev.params(200, 1e-4, 0.2, 1.0, tpm=tpm)
+    p1 = dev.params(iters, 1e-4, 1.0, 0.1, tpm=tpm, hist_mode=hist_mode)
+    p2 = dev.params(200, 1e-4, 0.2, 1.0, tpm=tpm, hist_mode=hist_mode)
     start = torch.from_numpy(x0).cuda()
     pos = torch.empty_like(start)
     it = torch.empty(C, dtype=torch.int32, device="cuda")
@@ -122,7 +122,7 @@ def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=N
 
     # DG + ETK on the device: the 3-D start is the collapsed 4-D result's first three coordinates
     edev = ETKDeviceBatch(b3)
-    p3 = edev.params(etk_iters, 1e-4, 0.0, 0.0, tpm=tpm)
+    p3 = edev.params(etk_iters, 1e-4, 0.0, 0.0, tpm=tpm, hist_mode=hist_mode)
     it3 = torch.empty(C, dtype=torch.int32, device="cuda")
 
     def dg_etk():
@@ -145,7 +145,7 @@ def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=N
     s3n, it3n = s3.cpu().numpy(), it3.cpu().numpy()
 
     out = {"workload": f"{n_mols}x{k} synthetic, heavy atoms 10-30", "conformers": C, "max_atoms": max_atoms,
-           "threads_per_conformer": tpm or "auto",
+           "threads_per_conformer": tpm or "auto", "history": ("auto", "shared", "device")[hist_mode],
            "dg_max_iters": iters, "seconds": t_dev, "conf_per_s": C / t_dev, "ms_per_conf": t_dev * 1e3 / C,
            "e2e_seconds": t_e2e, "e2e_conf_per_s": C / t_e2e, "converged": float(np.mean(s1n == 0)),
            "mean_iters": float(itn.mean()), "max_iters_hit": int(np.sum(itn >= iters)),
@@ -178,12 +178,14 @@ def main():
     ap.add_argument("--repeats", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--tpm", default="auto", help="threads per conformer: auto or a comma list of 32/64/128/256")
+    ap.add_argument("--history", default="0", help="L-BFGS history: comma list of 0 (auto) / 1 (shared) / 2 (device)")
     a = ap.parse_args()
     tpms = [None] if a.tpm == "auto" else [int(v) for v in a.tpm.split(",")]
     for w in a.workloads.split(","):
         n, k = (int(v) for v in w.split("x"))
         for tpm in tpms:
-            print(json.dumps(run(n, k, a.repeats, a.cpu_sample, tpm=tpm)), flush=True)
+            for hm in (int(v) for v in a.history.split(",")):
+                print(json.dumps(run(n, k, a.repeats, a.cpu_sample, tpm=tpm, hist_mode=hm)), flush=True)
 
 
 if __name__ == "__main__":

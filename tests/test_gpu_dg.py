@@ -128,3 +128,20 @@ def test_stereo_checks_match_the_reference(dg_golden):
                             [0, 1, 2], b.n_confs_total, dim=4)
     ref = dg_golden["sy_stereo_passed"]
     assert np.array_equal(got, ref) and (~ref).any() and ref.any()
+
+
+def test_history_placement_changes_nothing():
+    """The L-BFGS history in shared memory or in a device slot: the same arithmetic, bit-identical."""
+    import torch
+    from mlxmolkit_b200.conformer_metal import DGDeviceBatch
+    b, _ = _synth_batch(n_mols=3, k=3, seed=43, lo=10, hi=30)
+    x0 = init_random_positions(b, seed=12)
+    out = []
+    for hm in (1, 2):
+        dev = DGDeviceBatch(b)
+        pos = torch.from_numpy(x0.copy()).cuda()
+        e, s = dev.minimize_device(pos, dev.params(300, 1e-4, 1.0, 0.1, hist_mode=hm))
+        torch.cuda.synchronize()
+        out.append((pos.cpu().numpy(), e.cpu().numpy(), s.cpu().numpy()))
+    for a, c in zip(*out):
+        assert np.array_equal(a, c)
