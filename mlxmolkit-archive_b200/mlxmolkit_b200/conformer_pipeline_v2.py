@@ -111,14 +111,27 @@ def _recenter_bounds(b3, pos3: np.ndarray) -> None:
 
 
 def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight, chiral_weight, variant,
-                     seed: int = 42):
-    """DG -> collapse -> (ETK) on the GPU; returns per molecule a list of (N, 3) conformers, whether
-    each conformer's DG and ETK stages converged, and its DG + ETK energy (:333-341)."""
-    from .conformer_metal import dg_minimize_shared
+                     seed: int = 42, timings: Optional[dict] = None):
+    """DG -> retry -> stereo checks -> collapse -> (ETK) on the GPU, positions resident on the device
+    between the stages; returns per molecule a list of (N, 3) conformers, whether each conformer's
+    DG and ETK stages converged, and its DG + ETK energy (:333-341)."""
+    import torch
+    from .conformer_metal import DGDeviceBatch
     from .dg_extract import metric_matrix_positions, synth_dg_params
     from .etk_extract import synth_etk_params
-    from .etk_metal import etk_minimize_shared
+    from .etk_metal import ETKDeviceBatch
     from .shared_batch import add_etk_to_batch, pack_shared_dg_batch
+    from .stereo_checks import TetrahedralTable, stereo_check_device
+    tick = time.perf_counter()
+
+    def lap(name):
+        nonlocal tick
+        if timings is not None:
+            torch.cuda.synchronize()
+            now = time.perf_counter()
+            timings[name] = timings.get(name, 0.0) + now - tick
+            tick = now
+
     dgp = [synth_dg_params(m) for m in mols]
     b4 = pack_shared_dg_batch(dgp, ks, dim=4)
     C = b4.n_confs_total
@@ -127,37 +140,50 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
     dg_iters = dg_max_iters if dg_max_iters > 0 else _auto_iters(complexity, 300, 20.0)
     etk_iters = etk_max_iters if etk_max_iters > 0 else _auto_iters(complexity, 150, 10.0)
     x4 = metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=4)
-    out4, e4, s4 = dg_minimize_shared(b4, x4, max_iters=dg_iters, fourth_dim_weight=fourth_dim_weight,
-                                      chiral_weight=chiral_weight)
-    n_failed = int(np.sum(s4 != 0))
-    if 0 < n_failed < C:                                         # :186-200
-        out2, e2, s2 = dg_minimize_shared(b4, out4, max_iters=2 * dg_iters, fourth_dim_weight=fourth_dim_weight,
-                                          chiral_weight=chiral_weight)
-        for c in np.nonzero(s4 != 0)[0]:
-            if s2[c] == 0 or e2[c] < e4[c]:
-                a0, a1 = int(b4.conf_atom_starts[c]) * 4, int(b4.conf_atom_starts[c + 1]) * 4
-                out4[a0:a1] = out2[a0:a1]
-                e4[c], s4[c] = e2[c], s2[c]
-    from .stereo_checks import run_stereo_checks                   # :197-209: a failure is DG status 2
-    passed = run_stereo_checks(out4, dgp, mols, b4.conf_atom_starts, b4.conf_to_mol, list(range(len(mols))), C, dim=4)
-    s4 = np.where(passed, s4, 2).astype(np.int32)
-    col, _, _ = dg_minimize_shared(b4, out4, max_iters=200, fourth_dim_weight=1.0, chiral_weight=0.2)
-    pos3 = col.reshape(-1, 4)[:, :3].reshape(-1).copy()
-    e3, s3 = np.zeros(C, np.float32), np.zeros(C, np.int32)
+    lap("dg_host")
+    dev4 = DGDeviceBatch(b4)
+    pos4 = torch.from_numpy(x4).cuda()
+    e4, s4 = dev4.minimize_device(pos4, dev4.params(dg_iters, 1e-4, chiral_weight, fourth_dim_weight))
+    e4, s4 = e4[:C].clone(), s4[:C].clone()
+    failed = s4 != 0
+    n_failed = int(failed.sum().item())
+    if 0 < n_failed < C:                                         # :186-200, warm start from the first pass
+        pos2 = pos4.clone()
+        e2, s2 = dev4.minimize_device(pos2, dev4.params(2 * dg_iters, 1e-4, chiral_weight, fourth_dim_weight))
+        better = failed & ((s2[:C] == 0) | (e2[:C] < e4))
+        counts = torch.from_numpy(np.diff(np.asarray(b4.conf_atom_starts)).astype(np.int64) * 4).cuda()
+        mask = torch.repeat_interleave(better, counts)
+        pos4 = torch.where(mask, pos2, pos4)
+        e4 = torch.where(better, e2[:C], e4)
+        s4 = torch.where(better, s2[:C], s4)
+    passed = stereo_check_device(dev4, TetrahedralTable(mols), pos4)[:C]   # :197-209
+    s4 = torch.where(passed != 0, s4, torch.full_like(s4, 2))
+    dev4.minimize_device(pos4, dev4.params(200, 1e-4, 0.2, 1.0))            # collapse, :211-215
+    pos3 = pos4.view(-1, 4)[:, :3].contiguous().view(-1)
+    lap("dg_gpu")
+    e3 = torch.zeros(C, dtype=torch.float32, device="cuda")
+    s3 = torch.zeros(C, dtype=torch.int32, device="cuda")
     if variant != "DG":
         b3 = pack_shared_dg_batch(dgp, ks, dim=3)
         add_etk_to_batch(b3, [synth_etk_params(m, p.bounds_mat) for m, p in zip(mols, dgp)])
-        _recenter_bounds(b3, pos3)
-        pos3, e3, s3 = etk_minimize_shared(b3, pos3, max_iters=etk_iters)
-    confs, ok, energy, c = [], [], [], 0
+        _recenter_bounds(b3, pos3.cpu().numpy())
+        dev3 = ETKDeviceBatch(b3)
+        lap("etk_host")
+        e3, s3 = dev3.minimize_device(pos3, dev3.params(etk_iters, 1e-4, 0.0, 0.0))
+        e3, s3 = e3[:C], s3[:C]
+        lap("etk_gpu")
+    p3 = pos3.cpu().numpy()
+    ok = ((s4 == 0) & (s3 == 0)).cpu().numpy()
+    en = (e4.double() + e3.double()).cpu().numpy()
+    confs, oks, energy, c = [], [], [], 0
     for m, k in zip(mols, ks):
         n = m.GetNumAtoms()
-        confs.append([pos3[(int(b4.conf_atom_starts[c + j])) * 3:(int(b4.conf_atom_starts[c + j]) + n) * 3]
+        confs.append([p3[int(b4.conf_atom_starts[c + j]) * 3:(int(b4.conf_atom_starts[c + j]) + n) * 3]
                       .reshape(n, 3).astype(np.float64) for j in range(k)])
-        ok.append([bool(s4[c + j] == 0 and s3[c + j] == 0) for j in range(k)])
-        energy.append([float(e4[c + j]) + float(e3[c + j]) for j in range(k)])
+        oks.append([bool(v) for v in ok[c:c + k]])
+        energy.append([float(v) for v in en[c:c + k]])
         c += k
-    return confs, ok, energy
+    return confs, oks, energy
 
 
 def generate_conformers_nk(
@@ -176,9 +202,11 @@ def generate_conformers_nk(
     mmff_use_lbfgs: Optional[bool] = None,
     mmff_variant: str = "MMFF94",
     embed: str = "auto",
+    timings: Optional[dict] = None,
 ) -> PipelineResult:
     """N molecules x k conformers: embedding (DG + ETK on the GPU for ``synth`` molecules) and
-    MMFF94/94s refinement on the GPU when ``run_mmff``."""
+    MMFF94/94s refinement on the GPU when ``run_mmff``.  ``timings`` (additive), when a dict,
+    receives the seconds of the device embedding's host and GPU parts."""
     if embed not in ("auto", "device", "host"):
         raise ValueError("embed must be 'auto', 'device' or 'host'")
     t0 = time.time()
@@ -193,7 +221,7 @@ def generate_conformers_nk(
         confs, ok, en = _embed_on_device([smiles_list[i] for i in dev_idx], [int(ks[i]) for i in dev_idx],
                                          dg_max_iters=dg_max_iters, etk_max_iters=etk_max_iters,
                                          fourth_dim_weight=fourth_dim_weight, chiral_weight=chiral_weight,
-                                         variant=variant)
+                                         variant=variant, timings=timings)
         for j, i in enumerate(dev_idx):
             embedded[i] = (smiles_list[i], confs[j])
             dg_ok[i], dg_e[i] = ok[j], en[j]
@@ -205,6 +233,7 @@ def generate_conformers_nk(
                                converged=list(dg_ok[i]) if dg_ok[i] else [True] * len(xs))
                for i, (m, xs) in enumerate(embedded)]
     n_batches = 0
+    t_mmff = time.perf_counter()
     if run_mmff and N:
         params, ok = [], []
         for (mol, xs) in embedded:
@@ -248,5 +277,7 @@ def generate_conformers_nk(
                         conv = [a and b for a, b in zip(conv, dg_ok[i])]
                     results[i].converged = conv
                     cursor += k
+    if timings is not None and run_mmff:
+        timings["mmff"] = timings.get("mmff", 0.0) + time.perf_counter() - t_mmff
     return PipelineResult(molecules=results, total_conformers=sum(len(r.positions_3d) for r in results),
                           total_time=time.time() - t0, n_batches=max(n_batches, 1))

@@ -25,6 +25,7 @@ numbers.
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass
 from typing import Optional
 
@@ -119,18 +120,88 @@ def _metric_embed(bmat: np.ndarray, rng: np.random.Generator, dim: int) -> np.nd
     return np.stack(cols, axis=1).astype(np.float32)
 
 
-def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) -> np.ndarray:
-    """Metric-matrix initial coordinates of every conformer (flat, atom-major, float32)."""
-    rng = np.random.default_rng(seed)
+def _metric_embed_sequential(batch, bounds_mats, rng, dim, out, first: int) -> None:
     starts = np.asarray(batch.conf_atom_starts)
-    out = np.zeros(int(starts[-1]) * dim, np.float32)
-    for c in range(int(batch.n_confs_total)):
+    for c in range(first, int(batch.n_confs_total)):
         a0, a1 = int(starts[c]), int(starts[c + 1])
         bm = bounds_mats[int(batch.conf_to_mol[c])]
         if bm is None:
             out[a0 * dim:a1 * dim] = rng.standard_normal((a1 - a0) * dim).astype(np.float32)
         else:
             out[a0 * dim:a1 * dim] = _metric_embed(np.asarray(bm), rng, dim).reshape(-1)
+
+
+def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) -> np.ndarray:
+    """Metric-matrix initial coordinates of every conformer (flat, atom-major, float32).
+
+    The draws follow the reference's order conformer by conformer.  When every molecule has a
+    bounds matrix, the distances of all conformers are drawn at once and each molecule's
+    conformers are decomposed in one batched ``eigh``; that equals the sequential result as long
+    as no conformer needs the extra uniform column of a non-positive eigenvalue.  From the first
+    conformer that does, the rest is redone sequentially from the same generator state."""
+    rng = np.random.default_rng(seed)
+    starts = np.asarray(batch.conf_atom_starts)
+    C = int(batch.n_confs_total)
+    out = np.zeros(int(starts[-1]) * dim, np.float32)
+    mols = [int(m) for m in np.asarray(batch.conf_to_mol)[:C]]
+    if C == 0 or any(bounds_mats[m] is None for m in set(mols)) or \
+            any(np.asarray(bounds_mats[m]).shape[0] <= 1 for m in set(mols)):
+        _metric_embed_sequential(batch, bounds_mats, rng, dim, out, 0)
+        return out
+    npairs = [np.asarray(bounds_mats[m]).shape[0] * (np.asarray(bounds_mats[m]).shape[0] - 1) // 2 for m in mols]
+    u = rng.random(int(sum(npairs)))
+    offs = np.concatenate([[0], np.cumsum(npairs)])
+    runs, c = [], 0
+    while c < C:                                   # runs of consecutive conformers of one molecule
+        e = c
+        while e < C and mols[e] == mols[c]:
+            e += 1
+        runs.append((c, e))
+        c = e
+
+    def embed_run(run):
+        """The run's coordinates; returns the index of its first conformer that needs the extra
+        uniform column (C when none does)."""
+        c, e = run
+        bm = np.asarray(bounds_mats[mols[c]], dtype=np.float64)
+        n = bm.shape[0]
+        iu, ju = np.triu_indices(n, 1)
+        upper = bm[iu, ju]
+        lower = np.minimum(bm[ju, iu], upper)
+        d = lower[None, :] + u[offs[c]:offs[e]].reshape(e - c, -1) * (upper - lower)[None, :]
+        d2 = np.zeros((e - c, n, n))
+        d2[:, iu, ju] = d2[:, ju, iu] = d * d
+        gram = -0.5 * (d2 - d2.mean(axis=2, keepdims=True) - d2.mean(axis=1, keepdims=True)
+                       + d2.mean(axis=(1, 2), keepdims=True))
+        evals, evecs = np.linalg.eigh(gram)
+        for j in range(e - c):
+            top = np.argsort(evals[j])[::-1][:dim]
+            if np.any(evals[j][top] <= 0.0):
+                return c + j
+            a0 = int(starts[c + j])
+            out[a0 * dim:(a0 + n) * dim] = (evecs[j][:, top] * np.sqrt(evals[j][top])).astype(np.float32).reshape(-1)
+        return C
+
+    workers = min(len(runs), os.cpu_count() or 1, 16)
+    if workers > 1:
+        from concurrent.futures import ThreadPoolExecutor     # eigh releases the interpreter lock
+        try:                                                   # one BLAS thread per worker
+            from threadpoolctl import threadpool_limits
+            limit = threadpool_limits(1)
+        except ImportError:
+            limit = None
+        try:
+            with ThreadPoolExecutor(workers) as ex:
+                bad = min(ex.map(embed_run, runs))
+        finally:
+            if limit is not None:
+                limit.restore_original_limits()
+    else:
+        bad = min((embed_run(r) for r in runs), default=C)
+    if bad < C:                                    # the reference's sequence from the first extra draw on
+        rng = np.random.default_rng(seed)
+        rng.random(int(offs[bad]))
+        _metric_embed_sequential(batch, bounds_mats, rng, dim, out, bad)
     return out
 
 

@@ -145,13 +145,14 @@ def synth_etk_params(mol, bounds_mat: np.ndarray) -> ETKParams:
                     seen.add((a, d))
                     d14.append((a, d, lb(a, d), ub(a, d), DIST14_WEIGHT))
     topo = np.asarray(mol.distance_matrix())
-    for a in range(n):
-        for d in range(a + 1, n):
-            if topo[a, d] < 4 or (a, d) in seen:
-                continue
-            if ub(a, d) > 0 and lb(a, d) > 0:
-                seen.add((a, d))
-                d14.append((a, d, lb(a, d), ub(a, d), LONG_RANGE_WEIGHT))
+    iu, ju = np.triu_indices(n, 1)                 # row-major, as the reference's double loop
+    keep = (topo[iu, ju] >= 4) & (bm[iu, ju] > 0) & (bm[ju, iu] > 0)
+    if seen:
+        taken = np.zeros((n, n), dtype=bool)
+        taken[tuple(np.array(sorted(seen)).T)] = True
+        keep &= ~taken[iu, ju]
+    for a, d in zip(iu[keep].tolist(), ju[keep].tolist()):
+        d14.append((a, d, bm[d, a], bm[a, d], LONG_RANGE_WEIGHT))
 
     def mid(i, j):
         return 0.5 * (lb(i, j) + ub(i, j))
