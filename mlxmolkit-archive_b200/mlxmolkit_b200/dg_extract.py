@@ -116,7 +116,10 @@ def _metric_embed(bmat: np.ndarray, rng: np.random.Generator, dim: int) -> np.nd
     gram = -0.5 * (d2 - d2.mean(axis=1, keepdims=True) - d2.mean(axis=0, keepdims=True) + d2.mean())
     evals, evecs = np.linalg.eigh(gram)
     top = np.argsort(evals)[::-1][:dim]
-    cols = [evecs[:, k] * np.sqrt(evals[k]) if evals[k] > 0.0 else 1.0 - 2.0 * rng.random(n) for k in top]
+    # a non-positive eigenvalue -- or none at all, for fewer atoms than dimensions -- takes a
+    # uniform [-1, 1] column
+    cols = [evecs[:, top[k]] * np.sqrt(evals[top[k]]) if k < len(top) and evals[top[k]] > 0.0
+            else 1.0 - 2.0 * rng.random(n) for k in range(dim)]
     return np.stack(cols, axis=1).astype(np.float32)
 
 
@@ -176,7 +179,7 @@ def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) ->
         evals, evecs = np.linalg.eigh(gram)
         for j in range(e - c):
             top = np.argsort(evals[j])[::-1][:dim]
-            if np.any(evals[j][top] <= 0.0):
+            if len(top) < dim or np.any(evals[j][top] <= 0.0):
                 return c + j
             a0 = int(starts[c + j])
             out[a0 * dim:(a0 + n) * dim] = (evecs[j][:, top] * np.sqrt(evals[j][top])).astype(np.float32).reshape(-1)

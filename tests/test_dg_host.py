@@ -205,3 +205,51 @@ def test_tetrahedral_centres_match_the_reference(dg_golden):
         assert np.array_equal(got, ref), mi
         q = tetrahedral_quads(mol)
         assert np.array_equal(q, ref[1:5].T)
+
+
+def _sequential_starts(b, bms, seed, dim):
+    from mlxmolkit_b200.dg_extract import _metric_embed_sequential
+    out = np.zeros(int(b.conf_atom_starts[-1]) * dim, np.float32)
+    _metric_embed_sequential(b, bms, np.random.default_rng(seed), dim, out, 0)
+    return out
+
+
+def test_metric_starts_batched_equal_sequential_with_extra_draws(dg_golden):
+    """The batched start generator equals the one-conformer-at-a-time one, also when a conformer
+    needs the extra uniform columns: a 3-atom molecule has fewer eigenvalues than 4 dimensions, and
+    a molecule of two atoms at zero distance has no positive one."""
+    from mlxmolkit_b200.dg_extract import metric_matrix_positions
+    params = _golden_synth_params(dg_golden)
+    bms = [dg_golden[f"s{mi}_bounds_mat"] for mi in range(3)]
+    tiny = np.array([[0, 1.5, 2.5], [1.4, 0, 1.5], [2.4, 1.4, 0]])           # 3 atoms
+    flat = np.zeros((2, 2))                                                 # 2 atoms, zero bounds
+    extra = [all_pairs_dg(3), all_pairs_dg(2)]
+    b = pack_shared_dg_batch(params + extra, [2, 2, 1, 2, 2], dim=4)
+    allb = bms + [tiny, flat]
+    got = metric_matrix_positions(b, allb, seed=11, dim=4)
+    ref = _sequential_starts(b, allb, 11, 4)
+    assert np.array_equal(got, ref)
+    assert np.isfinite(got).all()
+
+
+def test_recentred_bounds_take_the_last_conformer(dg_golden):
+    """conformer_pipeline_v2.py:224-258: the 1-2 / 1-3 bounds move to the measured distances of the
+    molecule's last conformer, keeping their half-widths."""
+    from mlxmolkit_b200.conformer_pipeline_v2 import _recenter_bounds
+    from mlxmolkit_b200.etk_extract import synth_etk_params
+    from mlxmolkit_b200.shared_batch import add_etk_to_batch
+    params = _golden_synth_params(dg_golden)
+    mols = [dg_golden_mol(dg_golden, mi) for mi in range(3)]
+    b3 = pack_shared_dg_batch(params, [2, 3, 1], dim=3)
+    add_etk_to_batch(b3, [synth_etk_params(m, dg_golden[f"s{mi}_bounds_mat"]) for mi, m in enumerate(mols)])
+    hw = (b3.etk_dist12_ub - b3.etk_dist12_lb).copy() / 2
+    rng = np.random.default_rng(2)
+    pos = rng.normal(0, 2.0, int(b3.conf_atom_starts[-1]) * 3).astype(np.float32)
+    _recenter_bounds(b3, pos)
+    for m, last in ((0, 1), (1, 4), (2, 5)):
+        t0, t1 = b3.etk_dist12_term_starts[m], b3.etk_dist12_term_starts[m + 1]
+        a0 = int(b3.conf_atom_starts[last]) * 3
+        x = pos[a0:a0 + 3 * int(b3.mol_n_atoms[m])].reshape(-1, 3).astype(np.float64)
+        d = np.linalg.norm(x[b3.etk_dist12_idx1[t0:t1]] - x[b3.etk_dist12_idx2[t0:t1]], axis=1)
+        np.testing.assert_allclose(b3.etk_dist12_lb[t0:t1], d - hw[t0:t1], atol=1e-5)
+        np.testing.assert_allclose(b3.etk_dist12_ub[t0:t1], d + hw[t0:t1], atol=1e-5)
