@@ -10,7 +10,6 @@
 import numpy as np
 import pytest
 
-from helpers import dg_synth_params
 from mlxmolkit_b200 import synth
 from mlxmolkit_b200.conformer_metal import dg_minimize_shared
 from mlxmolkit_b200.dg_extract import DGParams, metric_matrix_positions, synth_dg_params
