@@ -34,6 +34,7 @@ MMFF stage (``run_mmff``), on the GPU:
 """
 from __future__ import annotations
 
+import os
 import time
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
@@ -87,6 +88,45 @@ def _embed(item, k: int, seed: int):
     return item, xyz[:k] if k else xyz
 
 
+# Term extraction is independent per molecule and runs in Python: batches of at least
+# _POOL_MIN molecules map it over a persistent pool of spawned host processes (spawn, so
+# that it is safe after CUDA has been initialised in this process).
+_POOL = None
+_POOL_MIN = 64
+
+
+def _pmap(fn, items):
+    global _POOL
+    workers = min(16, os.cpu_count() or 1)
+    if len(items) < _POOL_MIN or workers < 2:
+        return [fn(x) for x in items]
+    if _POOL is None:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        _POOL = ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn"))
+    return list(_POOL.map(fn, items, chunksize=max(1, len(items) // (4 * workers))))
+
+
+def _dg_terms(mol):
+    from .dg_extract import synth_dg_params
+    return synth_dg_params(mol)
+
+
+def _etk_terms(mol_and_bounds):
+    from .etk_extract import synth_etk_params
+    mol, bm = mol_and_bounds
+    return synth_etk_params(mol, bm)
+
+
+def _mmff_terms(mol_and_variant):
+    """MMFF parameters from the molecule's first conformer, or None when typing fails."""
+    mol, variant = mol_and_variant
+    try:
+        return extract_mmff_params(mol, conf_id=mol.GetConformers()[0].GetId(), mmff_variant=variant)
+    except Exception:
+        return None
+
+
 def _recenter_bounds(b3, pos3: np.ndarray) -> None:
     """Re-centre each molecule's 1-2 / 1-3 ETK bounds on the measured 3-D distances, keeping
     their half-widths (conformer_pipeline_v2.py:224-258; the last conformer of a molecule wins)."""
@@ -117,8 +157,7 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
     DG and ETK stages converged, and its DG + ETK energy (:333-341)."""
     import torch
     from .conformer_metal import DGDeviceBatch
-    from .dg_extract import metric_matrix_positions, synth_dg_params
-    from .etk_extract import synth_etk_params
+    from .dg_extract import metric_matrix_positions
     from .etk_metal import ETKDeviceBatch
     from .shared_batch import add_etk_to_batch, pack_shared_dg_batch
     from .stereo_checks import TetrahedralTable, stereo_check_device
@@ -132,7 +171,7 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
             timings[name] = timings.get(name, 0.0) + now - tick
             tick = now
 
-    dgp = [synth_dg_params(m) for m in mols]
+    dgp = _pmap(_dg_terms, list(mols))
     b4 = pack_shared_dg_batch(dgp, ks, dim=4)
     C = b4.n_confs_total
     max_atoms = max(p.n_atoms for p in dgp)
@@ -165,7 +204,7 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
     s3 = torch.zeros(C, dtype=torch.int32, device="cuda")
     if variant != "DG":
         b3 = pack_shared_dg_batch(dgp, ks, dim=3)
-        add_etk_to_batch(b3, [synth_etk_params(m, p.bounds_mat) for m, p in zip(mols, dgp)])
+        add_etk_to_batch(b3, _pmap(_etk_terms, [(m, p.bounds_mat) for m, p in zip(mols, dgp)]))
         _recenter_bounds(b3, pos3.cpu().numpy())
         dev3 = ETKDeviceBatch(b3)
         lap("etk_host")
@@ -235,15 +274,8 @@ def generate_conformers_nk(
     n_batches = 0
     t_mmff = time.perf_counter()
     if run_mmff and N:
-        params, ok = [], []
-        for (mol, xs) in embedded:
-            try:
-                params.append(extract_mmff_params(mol, conf_id=mol.GetConformers()[0].GetId(),
-                                                  mmff_variant=mmff_variant))
-                ok.append(len(xs) > 0)
-            except Exception:
-                params.append(None)
-                ok.append(False)
+        params = _pmap(_mmff_terms, [(mol, mmff_variant) for mol, _ in embedded])
+        ok = [p is not None and len(xs) > 0 for p, (_, xs) in zip(params, embedded)]
         for i, good in enumerate(ok):
             if not good:
                 results[i].converged = [False] * len(results[i].positions_3d)

@@ -253,3 +253,20 @@ def test_recentred_bounds_take_the_last_conformer(dg_golden):
         d = np.linalg.norm(x[b3.etk_dist12_idx1[t0:t1]] - x[b3.etk_dist12_idx2[t0:t1]], axis=1)
         np.testing.assert_allclose(b3.etk_dist12_lb[t0:t1], d - hw[t0:t1], atol=1e-5)
         np.testing.assert_allclose(b3.etk_dist12_ub[t0:t1], d + hw[t0:t1], atol=1e-5)
+
+
+def test_pooled_extraction_equals_in_process():
+    """generate_conformers_nk maps the per-molecule term extraction over spawned host processes for
+    large batches; the terms are the same as in-process."""
+    from dataclasses import fields
+
+    from mlxmolkit_b200 import conformer_pipeline_v2 as cp
+    from mlxmolkit_b200 import synth
+    mols = synth.make_molecules(cp._POOL_MIN, 1, 9, 8, 16, workers=1)
+    for fn, items in ((cp._dg_terms, mols), (cp._mmff_terms, [(m, "MMFF94s") for m in mols])):
+        serial = [fn(x) for x in items]
+        pooled = cp._pmap(fn, items)
+        for a, b in zip(serial, pooled):
+            for f in fields(a):
+                va, vb = getattr(a, f.name), getattr(b, f.name)
+                assert np.array_equal(np.asarray(va), np.asarray(vb)), f.name
