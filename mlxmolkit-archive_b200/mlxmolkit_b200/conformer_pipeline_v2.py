@@ -43,6 +43,7 @@ import numpy as np
 
 from . import mmff_minimize as mm
 from .mmff_params import extract_mmff_params
+from .pack import merge_packed
 
 
 @dataclass
@@ -119,12 +120,15 @@ def _etk_terms(mol_and_bounds):
 
 
 def _mmff_terms(mol_and_variant):
-    """MMFF parameters from the molecule's first conformer, or None when typing fails."""
+    """MMFF parameters from the molecule's first conformer and the molecule's packed tables, or
+    (None, None) when typing or packing fails."""
+    from .pack import pack_molecules
     mol, variant = mol_and_variant
     try:
-        return extract_mmff_params(mol, conf_id=mol.GetConformers()[0].GetId(), mmff_variant=variant)
+        p = extract_mmff_params(mol, conf_id=mol.GetConformers()[0].GetId(), mmff_variant=variant)
+        return p, pack_molecules([p])
     except Exception:
-        return None
+        return None, None
 
 
 def _recenter_bounds(b3, pos3: np.ndarray) -> None:
@@ -274,7 +278,8 @@ def generate_conformers_nk(
     n_batches = 0
     t_mmff = time.perf_counter()
     if run_mmff and N:
-        params = _pmap(_mmff_terms, [(mol, mmff_variant) for mol, _ in embedded])
+        terms = _pmap(_mmff_terms, [(mol, mmff_variant) for mol, _ in embedded])
+        params, packs = [t[0] for t in terms], [t[1] for t in terms]
         ok = [p is not None and len(xs) > 0 for p, (_, xs) in zip(params, embedded)]
         for i, good in enumerate(ok):
             if not good:
@@ -293,7 +298,8 @@ def generate_conformers_nk(
                 if not grp:
                     continue
                 n_batches += 1
-                m = mm.Minimizer([params[i] for i in grp], [len(embedded[i][1]) for i in grp])
+                m = mm.Minimizer([params[i] for i in grp], [len(embedded[i][1]) for i in grp],
+                                 packed=merge_packed([packs[i] for i in grp]))
                 pos = np.concatenate([np.stack(embedded[i][1]).reshape(-1) for i in grp]).astype(np.float32)
                 r = m.minimize(pos, max_iters=iters, grad_tol=1e-4, history_m=hist)
                 cursor = 0

@@ -151,10 +151,12 @@ class MinimizeResult:
 class Minimizer:
     """Device-resident minimisation of one packed batch (tables uploaded once)."""
 
-    def __init__(self, params_list, conf_counts: Sequence[int], device=None):
+    def __init__(self, params_list, conf_counts: Sequence[int], device=None, packed: Optional[PackedBatch] = None):
+        """``packed``: the molecules' tables when already packed (e.g. merged from per-molecule packs)."""
         self.params_list = list(params_list)
         self.conf_counts = [int(k) for k in conf_counts]
-        self.batch = DeviceBatch.from_params(self.params_list, device)
+        self.batch = DeviceBatch(packed, device) if packed is not None else \
+            DeviceBatch.from_params(self.params_list, device)
         n_atoms = [int(p.n_atoms) for p in self.params_list]
         self.conf_mol, self.conf_coord, self.total = conformer_index(n_atoms, self.conf_counts)
         self.order = lpt_order(n_atoms, self.conf_mol)

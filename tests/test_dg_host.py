@@ -263,10 +263,20 @@ def test_pooled_extraction_equals_in_process():
     from mlxmolkit_b200 import conformer_pipeline_v2 as cp
     from mlxmolkit_b200 import synth
     mols = synth.make_molecules(cp._POOL_MIN, 1, 9, 8, 16, workers=1)
-    for fn, items in ((cp._dg_terms, mols), (cp._mmff_terms, [(m, "MMFF94s") for m in mols])):
-        serial = [fn(x) for x in items]
-        pooled = cp._pmap(fn, items)
-        for a, b in zip(serial, pooled):
-            for f in fields(a):
-                va, vb = getattr(a, f.name), getattr(b, f.name)
-                assert np.array_equal(np.asarray(va), np.asarray(vb)), f.name
+    serial = [cp._dg_terms(m) for m in mols]
+    for a, b in zip(serial, cp._pmap(cp._dg_terms, mols)):
+        for f in fields(a):
+            assert np.array_equal(np.asarray(getattr(a, f.name)), np.asarray(getattr(b, f.name))), f.name
+    items = [(m, "MMFF94s") for m in mols]
+    serial = [cp._mmff_terms(x) for x in items]
+    pooled = cp._pmap(cp._mmff_terms, items)
+    for (pa, ka), (pb, kb) in zip(serial, pooled):
+        for f in fields(pa):
+            assert np.array_equal(np.asarray(getattr(pa, f.name)), np.asarray(getattr(pb, f.name))), f.name
+        for f in fields(ka):
+            assert np.array_equal(np.asarray(getattr(ka, f.name)), np.asarray(getattr(kb, f.name))), f.name
+    # the per-molecule packs merge into exactly the tables of packing the list at once
+    from mlxmolkit_b200.pack import merge_packed, pack_molecules
+    whole, merged = pack_molecules([p for p, _ in serial]), merge_packed([k for _, k in pooled])
+    for f in fields(whole):
+        assert np.array_equal(np.asarray(getattr(whole, f.name)), np.asarray(getattr(merged, f.name))), f.name
