@@ -19,18 +19,17 @@ Per workload it reports:
   * ``e2e_conf_per_s``: the same through ``dg_minimize_shared`` with host arrays
     (tables packed and uploaded, positions copied both ways, every call);
   * ``converged``: the fraction of conformers with status 0 after the 4-D stage;
-  * ``dg_etk_conf_per_s``: DG, collapse, 3-D extraction and ETK, all on the device;
-  * ``oracle``: agreement with the FP64 oracle on a sample of conformers
-    (statuses, and energies where both converged) and the oracle's own
-    conformers/s on all host threads.
+  * ``dg_etk_conf_per_s``: DG, collapse, 3-D extraction and ETK, all on the device.
 
-Usage: python -m mlxmolkit_b200.dg_bench [--workloads 20x50,1000x10] [--cpu-sample 64] [--tpm auto|32,64,...]
+The FP64 CPU baseline of the same stages is ``bench.py --workload dg``; agreement
+with the FP64 restatement is what tests/test_gpu_dg.py and tests/test_gpu_etk.py check.
+
+Usage: python -m mlxmolkit_b200.dg_bench [--workloads 20x50,1000x10] [--tpm auto|32,64,...]
 """
 from __future__ import annotations
 
 import argparse
 import json
-import os
 import time
 
 import numpy as np
@@ -60,7 +59,7 @@ def _workload(n_mols: int, k: int, seed: int):
 
 
 def _sub_batch(b, confs):
-    """The conformers ``confs`` of batch b as a batch of their own (for the oracle sample)."""
+    """The conformers ``confs`` of batch b as a batch of their own (a CPU baseline's sample)."""
     mols = sorted(set(int(b.conf_to_mol[c]) for c in confs))
     from .dg_extract import DGParams
     ps = []
@@ -77,7 +76,7 @@ def _sub_batch(b, confs):
     return pack_shared_dg_batch(ps, counts, dim=b.dim), ordered
 
 
-def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=None, hist_mode: int = 0) -> dict:
+def run(n_mols: int, k: int, repeats: int, seed: int = 0, tpm=None, hist_mode: int = 0) -> dict:
     import torch
     b4, x0, iters, max_atoms, b3, etk_iters = _workload(n_mols, k, seed)
     C = b4.n_confs_total
@@ -151,24 +150,6 @@ def run(n_mols: int, k: int, repeats: int, cpu_sample: int, seed: int = 0, tpm=N
            "mean_iters": float(itn.mean()), "max_iters_hit": int(np.sum(itn >= iters)),
            "etk_max_iters": etk_iters, "dg_etk_seconds": t_dg_etk, "dg_etk_conf_per_s": C / t_dg_etk,
            "etk_converged": float(np.mean(s3n == 0)), "etk_mean_iters": float(it3n.mean())}
-    if cpu_sample:
-        from oracle import dg as odg
-        rng = np.random.default_rng(1)
-        confs = sorted(rng.choice(C, min(cpu_sample, C), replace=False).tolist())
-        sb, order = _sub_batch(b4, confs)
-        xs = np.concatenate([x0[int(b4.conf_atom_starts[c]) * 4:int(b4.conf_atom_starts[c + 1]) * 4] for c in order])
-        threads = os.cpu_count() or 1
-        t = time.perf_counter()
-        _, eo, so, _ = odg.minimize(sb, xs, max_iters=iters, chiral_weight=1.0, fourth_dim_weight=0.1,
-                                    threads=threads)
-        t_cpu = time.perf_counter() - t
-        _, eg, sg = dg_minimize_shared(sb, xs, max_iters=iters, chiral_weight=1.0, fourth_dim_weight=0.1)
-        both = (sg == 0) & (so == 0)
-        out["oracle"] = {"sample": len(order), "status_agree": float(np.mean(sg == so)),
-                         "energy_agree_both_converged": float(np.mean(np.abs(eg[both] - eo[both]) <=
-                                                                     1e-3 * np.maximum(1.0, np.abs(eo[both]))))
-                         if both.any() else None,
-                         "cpu_threads": threads, "cpu_conf_per_s_4d_stage": len(order) / t_cpu}
     return out
 
 
@@ -176,7 +157,6 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workloads", default="20x50,1000x10")
     ap.add_argument("--repeats", type=int, default=5)
-    ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--tpm", default="auto", help="threads per conformer: auto or a comma list of 32/64/128/256")
     ap.add_argument("--history", default="0", help="L-BFGS history: comma list of 0 (auto) / 1 (shared) / 2 (device)")
     a = ap.parse_args()
@@ -185,7 +165,7 @@ def main():
         n, k = (int(v) for v in w.split("x"))
         for tpm in tpms:
             for hm in (int(v) for v in a.history.split(",")):
-                print(json.dumps(run(n, k, a.repeats, a.cpu_sample, tpm=tpm, hist_mode=hm)), flush=True)
+                print(json.dumps(run(n, k, a.repeats, tpm=tpm, hist_mode=hm)), flush=True)
 
 
 if __name__ == "__main__":
