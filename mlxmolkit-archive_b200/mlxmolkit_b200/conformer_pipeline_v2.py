@@ -256,6 +256,9 @@ def generate_conformers_nk(
     N = len(smiles_list)
     ks = [n_confs_per_mol] * N if isinstance(n_confs_per_mol, int) else list(n_confs_per_mol)
     on_device = [embed == "device" or (embed == "auto" and hasattr(item, "distance_matrix")) for item in smiles_list]
+    if embed == "device" and not all(hasattr(item, "distance_matrix") for item in smiles_list):
+        raise ValueError("embed='device' needs synth molecules: their bounds matrices come from the stand-in "
+                         "extraction (RDKit's bounds matrix is not available)")
     embedded = [None] * N
     dg_ok = [None] * N
     dg_e = [None] * N

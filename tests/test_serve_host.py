@@ -30,3 +30,12 @@ def test_topology_key_separates_graphs_types_and_variants():
     c = a.copy()
     c.types[0] = "XX"
     assert ka != serve.topology_key(c, "MMFF94")
+
+
+def test_generate_conformers_nk_rejects_bad_embed_arguments():
+    import pytest as _pytest
+    from mlxmolkit_b200.conformer_pipeline_v2 import generate_conformers_nk
+    with _pytest.raises(ValueError):
+        generate_conformers_nk(["CCO"], 2, embed="bogus")
+    with _pytest.raises(ValueError):
+        generate_conformers_nk(["CCO"], 2, embed="device")      # a SMILES string has no bounds here
