@@ -96,21 +96,113 @@ _POOL = None
 _POOL_MIN = 64
 
 
-def _pmap(fn, items):
+def _pool_for(n_items: int):
+    """The process pool when a batch of ``n_items`` molecules uses it, else None."""
     global _POOL
     workers = min(16, os.cpu_count() or 1)
-    if len(items) < _POOL_MIN or workers < 2:
-        return [fn(x) for x in items]
+    if n_items < _POOL_MIN or workers < 2:
+        return None
     if _POOL is None:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
         _POOL = ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn"))
-    return list(_POOL.map(fn, items, chunksize=max(1, len(items) // (4 * workers))))
+    return _POOL
+
+
+def _chunk(n_items: int) -> int:
+    return max(1, n_items // (4 * min(16, os.cpu_count() or 1)))
+
+
+def _pmap(fn, items):
+    pool = _pool_for(len(items))
+    if pool is None:
+        return [fn(x) for x in items]
+    return list(pool.map(fn, items, chunksize=_chunk(len(items))))
+
+
+def _pmap_async(fn, items):
+    """Queue ``fn`` over ``items`` on the pool now (in-process at the call, for small batches);
+    returns a function that waits for and returns the results."""
+    pool = _pool_for(len(items))
+    if pool is None:
+        return lambda: [fn(x) for x in items]
+    it = pool.map(fn, items, chunksize=_chunk(len(items)))
+    return lambda: list(it)
 
 
 def _dg_terms(mol):
     from .dg_extract import synth_dg_params
     return synth_dg_params(mol)
+
+
+_ONE_BLAS_THREAD = None
+
+
+def _dg_terms_and_starts(item):
+    """A molecule's DG terms and the metric-matrix starts of its k conformers, from its slice of
+    the batch's draw sequence (``dg_extract.embed_conformers``): (params, (k, n * dim) float32,
+    index of the first conformer that needs an extra uniform column, k when none), or
+    (params, None, 0) for a molecule the batched form does not cover."""
+    global _ONE_BLAS_THREAD
+    from .dg_extract import embed_conformers, synth_dg_params, uniform_draws
+    if _ONE_BLAS_THREAD is None:                  # the pool's processes share the cores
+        try:
+            from threadpoolctl import threadpool_limits
+            _ONE_BLAS_THREAD = threadpool_limits(1)
+        except ImportError:
+            _ONE_BLAS_THREAD = False
+    mol, k, seed, offset, dim = item
+    p = synth_dg_params(mol)
+    n = int(p.n_atoms)
+    if p.bounds_mat is None or n <= 1 or k == 0:
+        return p, None, 0
+    xyz, j = embed_conformers(p.bounds_mat, uniform_draws(seed, offset, k * n * (n - 1) // 2), k, dim)
+    return p, xyz, j
+
+
+def _dg_terms_and_positions(mols, ks, seed: int, dim: int = 4):
+    """DG terms, the packed batch and its metric-matrix starts (``metric_matrix_positions``'s
+    result); on the process pool for large batches, each task one molecule's terms and starts."""
+    from .dg_extract import metric_matrix_positions, pair_draw_offsets
+    from .shared_batch import pack_shared_dg_batch
+    if _pool_for(len(mols)) is None:
+        dgp = [_dg_terms(m) for m in mols]
+        b4 = pack_shared_dg_batch(dgp, ks, dim=dim)
+        return dgp, b4, metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=dim)
+    first = np.concatenate([[0], np.cumsum(ks)]).astype(np.int64)
+    offs = pair_draw_offsets(np.repeat([m.GetNumAtoms() for m in mols], ks))
+    res = _pmap(_dg_terms_and_starts, [(m, int(k), seed, int(offs[first[i]]), dim)
+                                       for i, (m, k) in enumerate(zip(mols, ks))])
+    dgp = [r[0] for r in res]
+    b4 = pack_shared_dg_batch(dgp, ks, dim=dim)
+    bounds = [p.bounds_mat for p in dgp]
+    out = _assemble_starts(res, ks, b4, seed, dim)
+    return dgp, b4, out if out is not None else metric_matrix_positions(b4, bounds, seed=seed, dim=dim)
+
+
+def _assemble_starts(res, ks, b4, seed: int, dim: int):
+    """The batch's starts from the per-molecule results of ``_dg_terms_and_starts``, equal to
+    ``metric_matrix_positions``; None when a molecule needs that function's sequential form."""
+    from .dg_extract import finish_sequentially
+    if any(r[1] is None for r, k in zip(res, ks) if k > 0) or \
+            not np.array_equal(np.diff(np.asarray(b4.conf_atom_starts)), np.repeat([r[0].n_atoms for r in res], ks)):
+        return None
+    first = np.concatenate([[0], np.cumsum(ks)]).astype(np.int64)
+    starts = np.asarray(b4.conf_atom_starts)
+    C = int(b4.n_confs_total)
+    out = np.zeros(int(starts[-1]) * dim, np.float32)
+    bad = C
+    for i, (_, xyz, j) in enumerate(res):
+        c0 = int(first[i])
+        if xyz is None:
+            continue
+        out[int(starts[c0]) * dim:int(starts[c0 + j]) * dim] = xyz[:j].reshape(-1)
+        if j < xyz.shape[0]:                       # later conformers' draws shift: redo from here
+            bad = c0 + j
+            break
+    if bad < C:
+        finish_sequentially(b4, [r[0].bounds_mat for r in res], seed, dim, out, bad)
+    return out
 
 
 def _etk_terms(mol_and_bounds):
@@ -155,13 +247,13 @@ def _recenter_bounds(b3, pos3: np.ndarray) -> None:
 
 
 def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight, chiral_weight, variant,
-                     seed: int = 42, timings: Optional[dict] = None):
+                     seed: int = 42, timings: Optional[dict] = None, after_host=None):
     """DG -> retry -> stereo checks -> collapse -> (ETK) on the GPU, positions resident on the device
     between the stages; returns per molecule a list of (N, 3) conformers, whether each conformer's
-    DG and ETK stages converged, and its DG + ETK energy (:333-341)."""
+    DG and ETK stages converged, its DG + ETK energy (:333-341), and what ``after_host`` -- called
+    once the stages' own host work is queued, before the first launch -- returned."""
     import torch
     from .conformer_metal import DGDeviceBatch
-    from .dg_extract import metric_matrix_positions
     from .etk_metal import ETKDeviceBatch
     from .shared_batch import add_etk_to_batch, pack_shared_dg_batch
     from .stereo_checks import TetrahedralTable, stereo_check_device
@@ -175,20 +267,35 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
             timings[name] = timings.get(name, 0.0) + now - tick
             tick = now
 
-    dgp = _pmap(_dg_terms, list(mols))
-    b4 = pack_shared_dg_batch(dgp, ks, dim=4)
+    dgp, b4, x4 = _dg_terms_and_positions(list(mols), ks, seed, dim=4)
+    if variant != "DG":                          # extracted on the pool while the GPU runs DG
+        etk_terms = _pmap_async(_etk_terms, [(m, p.bounds_mat) for m, p in zip(mols, dgp)])
+    background = after_host() if after_host is not None else None
     C = b4.n_confs_total
     max_atoms = max(p.n_atoms for p in dgp)
     complexity = max(max_atoms, int(max(len(p.dist_idx1) for p in dgp) ** 0.5))
     dg_iters = dg_max_iters if dg_max_iters > 0 else _auto_iters(complexity, 300, 20.0)
     etk_iters = etk_max_iters if etk_max_iters > 0 else _auto_iters(complexity, 150, 10.0)
-    x4 = metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=4)
     lap("dg_host")
     dev4 = DGDeviceBatch(b4)
     pos4 = torch.from_numpy(x4).cuda()
     e4, s4 = dev4.minimize_device(pos4, dev4.params(dg_iters, 1e-4, chiral_weight, fourth_dim_weight))
     e4, s4 = e4[:C].clone(), s4[:C].clone()
     failed = s4 != 0
+    # while the GPU runs DG: the stereo table and the ETK tables, built here and uploaded on a
+    # side stream (a copy on this stream would wait for DG); the ETK bounds are patched in once
+    # they are re-centred on the 3-D distances
+    main, side = torch.cuda.current_stream(), torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        tet = TetrahedralTable(mols)
+        dev3 = None
+        if variant != "DG":
+            b3 = pack_shared_dg_batch(dgp, ks, dim=3)
+            add_etk_to_batch(b3, etk_terms())
+            dev3 = ETKDeviceBatch(b3)
+    main.wait_stream(side)
+    for t in [tet.starts, tet.quads] + (list(dev3.dev.values()) if dev3 is not None else []):
+        t.record_stream(main)
     n_failed = int(failed.sum().item())
     if 0 < n_failed < C:                                         # :186-200, warm start from the first pass
         pos2 = pos4.clone()
@@ -199,7 +306,7 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
         pos4 = torch.where(mask, pos2, pos4)
         e4 = torch.where(better, e2[:C], e4)
         s4 = torch.where(better, s2[:C], s4)
-    passed = stereo_check_device(dev4, TetrahedralTable(mols), pos4)[:C]   # :197-209
+    passed = stereo_check_device(dev4, tet, pos4)[:C]                     # :197-209
     s4 = torch.where(passed != 0, s4, torch.full_like(s4, 2))
     dev4.minimize_device(pos4, dev4.params(200, 1e-4, 0.2, 1.0))            # collapse, :211-215
     pos3 = pos4.view(-1, 4)[:, :3].contiguous().view(-1)
@@ -207,10 +314,8 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
     e3 = torch.zeros(C, dtype=torch.float32, device="cuda")
     s3 = torch.zeros(C, dtype=torch.int32, device="cuda")
     if variant != "DG":
-        b3 = pack_shared_dg_batch(dgp, ks, dim=3)
-        add_etk_to_batch(b3, _pmap(_etk_terms, [(m, p.bounds_mat) for m, p in zip(mols, dgp)]))
         _recenter_bounds(b3, pos3.cpu().numpy())
-        dev3 = ETKDeviceBatch(b3)
+        dev3.refresh_bounds()
         lap("etk_host")
         e3, s3 = dev3.minimize_device(pos3, dev3.params(etk_iters, 1e-4, 0.0, 0.0))
         e3, s3 = e3[:C], s3[:C]
@@ -226,7 +331,7 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
         oks.append([bool(v) for v in ok[c:c + k]])
         energy.append([float(v) for v in en[c:c + k]])
         c += k
-    return confs, oks, energy
+    return confs, oks, energy, background
 
 
 def generate_conformers_nk(
@@ -263,11 +368,18 @@ def generate_conformers_nk(
     dg_ok = [None] * N
     dg_e = [None] * N
     dev_idx = [i for i in range(N) if on_device[i]]
+    # molecules that carry their own conformer are MMFF-typed from it whatever the embedding, so
+    # their extraction is queued behind the embedding's host work and runs during its GPU stages
+    pre_idx = [i for i in range(N) if not isinstance(smiles_list[i], str)] if run_mmff else []
+    pre_terms = None
     if dev_idx:
-        confs, ok, en = _embed_on_device([smiles_list[i] for i in dev_idx], [int(ks[i]) for i in dev_idx],
-                                         dg_max_iters=dg_max_iters, etk_max_iters=etk_max_iters,
-                                         fourth_dim_weight=fourth_dim_weight, chiral_weight=chiral_weight,
-                                         variant=variant, timings=timings)
+        def queue_mmff():
+            return _pmap_async(_mmff_terms, [(smiles_list[i], mmff_variant) for i in pre_idx]) if pre_idx else None
+
+        confs, ok, en, pre_terms = _embed_on_device(
+            [smiles_list[i] for i in dev_idx], [int(ks[i]) for i in dev_idx], dg_max_iters=dg_max_iters,
+            etk_max_iters=etk_max_iters, fourth_dim_weight=fourth_dim_weight, chiral_weight=chiral_weight,
+            variant=variant, timings=timings, after_host=queue_mmff)
         for j, i in enumerate(dev_idx):
             embedded[i] = (smiles_list[i], confs[j])
             dg_ok[i], dg_e[i] = ok[j], en[j]
@@ -281,7 +393,13 @@ def generate_conformers_nk(
     n_batches = 0
     t_mmff = time.perf_counter()
     if run_mmff and N:
-        terms = _pmap(_mmff_terms, [(mol, mmff_variant) for mol, _ in embedded])
+        terms = [None] * N
+        if pre_terms is not None:
+            for i, t in zip(pre_idx, pre_terms()):
+                terms[i] = t
+        rest = [i for i in range(N) if terms[i] is None]
+        for i, t in zip(rest, _pmap(_mmff_terms, [(embedded[i][0], mmff_variant) for i in rest])):
+            terms[i] = t
         params, packs = [t[0] for t in terms], [t[1] for t in terms]
         ok = [p is not None and len(xs) > 0 for p, (_, xs) in zip(params, embedded)]
         for i, good in enumerate(ok):

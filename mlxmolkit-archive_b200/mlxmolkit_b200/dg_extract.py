@@ -134,6 +134,54 @@ def _metric_embed_sequential(batch, bounds_mats, rng, dim, out, first: int) -> N
             out[a0 * dim:a1 * dim] = _metric_embed(np.asarray(bm), rng, dim).reshape(-1)
 
 
+def uniform_draws(seed: int, offset: int, count: int) -> np.ndarray:
+    """Draws ``offset`` .. ``offset + count`` of ``np.random.default_rng(seed).random``, without
+    drawing the ones before (the PCG64 state jumped ahead; one 64-bit step per double)."""
+    bg = np.random.PCG64(seed)
+    bg.advance(int(offset))
+    return np.random.Generator(bg).random(int(count))
+
+
+def embed_conformers(bmat: np.ndarray, u: np.ndarray, k: int, dim: int):
+    """Metric-matrix coordinates of ``k`` conformers of one molecule in one batched ``eigh``,
+    from their ``k * n(n-1)/2`` uniform distance draws ``u`` (conformer-major, row-major upper
+    triangle).  Returns ((k, n * dim) float32, j): j is the first conformer that needs the extra
+    uniform column of a non-positive eigenvalue (k when none does); rows from j on are unset."""
+    bm = np.asarray(bmat, dtype=np.float64)
+    n = bm.shape[0]
+    iu, ju = np.triu_indices(n, 1)
+    upper = bm[iu, ju]
+    lower = np.minimum(bm[ju, iu], upper)
+    d = lower[None, :] + np.asarray(u).reshape(k, -1) * (upper - lower)[None, :]
+    d2 = np.zeros((k, n, n))
+    d2[:, iu, ju] = d2[:, ju, iu] = d * d
+    gram = -0.5 * (d2 - d2.mean(axis=2, keepdims=True) - d2.mean(axis=1, keepdims=True)
+                   + d2.mean(axis=(1, 2), keepdims=True))
+    evals, evecs = np.linalg.eigh(gram)
+    out = np.zeros((k, n * dim), np.float32)
+    for j in range(k):
+        top = np.argsort(evals[j])[::-1][:dim]
+        if len(top) < dim or np.any(evals[j][top] <= 0.0):
+            return out, j
+        out[j] = (evecs[j][:, top] * np.sqrt(evals[j][top])).astype(np.float32).reshape(-1)
+    return out, k
+
+
+def pair_draw_offsets(n_atoms_per_conf) -> np.ndarray:
+    """Start of each conformer's distance draws in the batch's draw sequence (length C + 1)."""
+    n = np.asarray(n_atoms_per_conf, dtype=np.int64)
+    return np.concatenate([[0], np.cumsum(n * (n - 1) // 2)])
+
+
+def finish_sequentially(batch, bounds_mats, seed: int, dim: int, out: np.ndarray, first: int) -> None:
+    """The reference's sequence from conformer ``first`` on, when that conformer needs an extra
+    uniform column: the generator is set to its state before that conformer's draws."""
+    offs = pair_draw_offsets(np.diff(np.asarray(batch.conf_atom_starts)))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rng.bit_generator.advance(int(offs[first]))
+    _metric_embed_sequential(batch, bounds_mats, rng, dim, out, first)
+
+
 def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) -> np.ndarray:
     """Metric-matrix initial coordinates of every conformer (flat, atom-major, float32).
 
@@ -151,9 +199,8 @@ def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) ->
             any(np.asarray(bounds_mats[m]).shape[0] <= 1 for m in set(mols)):
         _metric_embed_sequential(batch, bounds_mats, rng, dim, out, 0)
         return out
-    npairs = [np.asarray(bounds_mats[m]).shape[0] * (np.asarray(bounds_mats[m]).shape[0] - 1) // 2 for m in mols]
-    u = rng.random(int(sum(npairs)))
-    offs = np.concatenate([[0], np.cumsum(npairs)])
+    offs = pair_draw_offsets(np.diff(starts[:C + 1]))
+    u = rng.random(int(offs[-1]))
     runs, c = [], 0
     while c < C:                                   # runs of consecutive conformers of one molecule
         e = c
@@ -163,27 +210,12 @@ def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) ->
         c = e
 
     def embed_run(run):
-        """The run's coordinates; returns the index of its first conformer that needs the extra
-        uniform column (C when none does)."""
+        """Writes the run's coordinates; returns the index of its first conformer that needs the
+        extra uniform column (C when none does)."""
         c, e = run
-        bm = np.asarray(bounds_mats[mols[c]], dtype=np.float64)
-        n = bm.shape[0]
-        iu, ju = np.triu_indices(n, 1)
-        upper = bm[iu, ju]
-        lower = np.minimum(bm[ju, iu], upper)
-        d = lower[None, :] + u[offs[c]:offs[e]].reshape(e - c, -1) * (upper - lower)[None, :]
-        d2 = np.zeros((e - c, n, n))
-        d2[:, iu, ju] = d2[:, ju, iu] = d * d
-        gram = -0.5 * (d2 - d2.mean(axis=2, keepdims=True) - d2.mean(axis=1, keepdims=True)
-                       + d2.mean(axis=(1, 2), keepdims=True))
-        evals, evecs = np.linalg.eigh(gram)
-        for j in range(e - c):
-            top = np.argsort(evals[j])[::-1][:dim]
-            if len(top) < dim or np.any(evals[j][top] <= 0.0):
-                return c + j
-            a0 = int(starts[c + j])
-            out[a0 * dim:(a0 + n) * dim] = (evecs[j][:, top] * np.sqrt(evals[j][top])).astype(np.float32).reshape(-1)
-        return C
+        xyz, j = embed_conformers(bounds_mats[mols[c]], u[offs[c]:offs[e]], e - c, dim)
+        out[int(starts[c]) * dim:int(starts[c + j]) * dim] = xyz[:j].reshape(-1)
+        return c + j if j < e - c else C
 
     workers = min(len(runs), os.cpu_count() or 1, 16)
     if workers > 1:
@@ -202,9 +234,7 @@ def metric_matrix_positions(batch, bounds_mats, seed: int = 42, dim: int = 4) ->
     else:
         bad = min((embed_run(r) for r in runs), default=C)
     if bad < C:                                    # the reference's sequence from the first extra draw on
-        rng = np.random.default_rng(seed)
-        rng.random(int(offs[bad]))
-        _metric_embed_sequential(batch, bounds_mats, rng, dim, out, bad)
+        finish_sequentially(batch, bounds_mats, seed, dim, out, bad)
     return out
 
 

@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _lib
 from .conformer_metal import DEFAULT_LBFGS_M, DGDeviceBatch, _torch
-from .shared_batch import SharedConstraintBatch, etk_device_arrays
+from .shared_batch import SharedConstraintBatch, etk_device_arrays, fb_bounds_patch
 
 
 class ETKDeviceBatch(DGDeviceBatch):
@@ -27,9 +27,11 @@ class ETKDeviceBatch(DGDeviceBatch):
     _ETK_INT = ("fb_starts", "fbinc_starts", "tor_starts", "tor_quads", "tinc_starts", "tinc_rec")
     _ETK_FLOAT = ("fb_rec", "fbinc_rec", "tor_coef")
 
-    def __init__(self, batch: SharedConstraintBatch, device: str = "cuda"):
+    def __init__(self, batch: SharedConstraintBatch, device: str = "cuda", arrays: Optional[dict] = None):
+        """``arrays``: the batch's ``etk_device_arrays``, when already built."""
         torch = _torch()
-        arrs = etk_device_arrays(batch)
+        arrs = arrays if arrays is not None else etk_device_arrays(batch)
+        self._placement = {f: arrs[f] for f in ("fb_row", "fbinc_pos", "fb_rec")}
         self.batch = batch
         self.n_conf = int(batch.n_confs_total)
         self.dim = 3
@@ -49,6 +51,19 @@ class ETKDeviceBatch(DGDeviceBatch):
         self.terms = _lib.MMFFETKTermsDev(max_tor=int(arrs["max_tor"]),
                                           **{f: self.dev[f].data_ptr() for f in self._ETK_INT + self._ETK_FLOAT})
         self._scratch = None
+
+    def refresh_bounds(self, tags=("12", "13")) -> None:
+        """Write the batch's current lower / upper bounds of the ``tags`` flat-bottom families into
+        the device tables (their term lists unchanged), on the current stream: the pipeline
+        re-centres the 1-2 / 1-3 bounds after the tables were uploaded."""
+        torch = _torch()
+        rows, inc_rows, vals = fb_bounds_patch(self._placement, self.batch, tags)
+        if len(rows) == 0:
+            return
+        dev = self.dev["fb_rec"].device
+        v = torch.from_numpy(vals).to(dev)
+        self.dev["fb_rec"][torch.from_numpy(rows).to(dev), 1:3] = v
+        self.dev["fbinc_rec"][torch.from_numpy(inc_rows).to(dev), 1:3] = torch.cat([v, v])
 
     def scratch(self, prm: _lib.MMFFDGParams):
         torch = _torch()

@@ -144,6 +144,27 @@ def _term_mol(starts: np.ndarray) -> np.ndarray:
     return np.repeat(np.arange(len(starts) - 1, dtype=np.int64), np.diff(starts))
 
 
+def _stable_order(row: np.ndarray) -> np.ndarray:
+    """The stable sorting permutation of ``row`` (non-negative int64): an unstable sort of the
+    unique keys row * len + position, which is the same permutation and faster."""
+    n = len(row)
+    if n == 0 or int(row.max()) >= (1 << 62) // n:
+        return np.argsort(row, kind="stable")
+    return np.argsort(row * n + np.arange(n, dtype=np.int64))
+
+
+def _incidence_rows(rec: np.ndarray, i1: np.ndarray, i2: np.ndarray, row: np.ndarray):
+    """Each 16-byte pair record under both of its atoms, in ``row`` order (term order within a
+    row), its first word replaced by the other atom's index; and the permutation used (incidence
+    row p holds record order[p] mod len(rec))."""
+    m = len(rec)
+    both = np.concatenate([rec, rec])
+    both[:m, 0] = i2.astype(np.int32).view(np.float32)
+    both[m:, 0] = i1.astype(np.int32).view(np.float32)
+    order = _stable_order(row)
+    return both[order], order
+
+
 def dg_device_arrays(batch: SharedConstraintBatch) -> dict:
     """The device layout of include/mmffb200_dg.h as numpy arrays (validated)."""
     if batch.dim not in (3, 4):
@@ -168,15 +189,9 @@ def dg_device_arrays(batch: SharedConstraintBatch) -> dict:
     dist_rec = np.empty((len(i1), 4), dtype=np.float32)
     dist_rec[:, 0] = (i1 | (i2 << 16)).astype(np.int32).view(np.float32)
     dist_rec[:, 1], dist_rec[:, 2], dist_rec[:, 3] = lb2, ub2, w
-    # every distance term under both of its atoms; a stable sort keeps term order within a row
+    # every distance term under both of its atoms, term order kept within a row
     row = np.concatenate([base[dm] + i1, base[dm] + i2])
-    other = np.concatenate([i2, i1])
-    order = np.argsort(row, kind="stable")
-    dinc_rec = np.empty((len(row), 4), dtype=np.float32)
-    dinc_rec[:, 0] = other[order].astype(np.int32).view(np.float32)
-    dinc_rec[:, 1] = np.concatenate([lb2, lb2])[order]
-    dinc_rec[:, 2] = np.concatenate([ub2, ub2])[order]
-    dinc_rec[:, 3] = np.concatenate([w, w])[order]
+    dinc_rec, _ = _incidence_rows(dist_rec, i1, i2, row)
     dinc_starts = _starts(np.bincount(row, minlength=rows)[:rows])
 
     cs = np.asarray(batch.chiral_term_starts, dtype=np.int64)
@@ -191,7 +206,7 @@ def dg_device_arrays(batch: SharedConstraintBatch) -> dict:
     crow = (base[cm][:, None] + quads).reshape(-1)
     cterm = np.repeat(np.arange(len(quads), dtype=np.int64), 4)
     crole = np.tile(np.arange(4, dtype=np.int64), len(quads))
-    corder = np.argsort(crow, kind="stable")
+    corder = _stable_order(crow)
     cinc_rec = np.stack([cterm[corder], crole[corder]], axis=1).astype(np.int32) if len(crow) \
         else np.zeros((0, 2), np.int32)
     cinc_starts = _starts(np.bincount(crow, minlength=rows)[:rows])
@@ -261,7 +276,8 @@ def _atoms_and_base(batch):
 
 
 def _pair_tables(starts, i1, i2, a, b, w, n_atoms, base, rows, what):
-    """16-byte pair records {i | j << 16, a, b, w} and their per-atom incidence rows."""
+    """16-byte pair records {i | j << 16, a, b, w}, their per-atom incidence rows, and the
+    incidence permutation (``_incidence_rows``)."""
     starts = np.asarray(starts, dtype=np.int64)
     tm = _term_mol(starts)
     i1 = np.asarray(i1, dtype=np.int64)
@@ -272,12 +288,8 @@ def _pair_tables(starts, i1, i2, a, b, w, n_atoms, base, rows, what):
     rec[:, 0] = (i1 | (i2 << 16)).astype(np.int32).view(np.float32)
     rec[:, 1], rec[:, 2], rec[:, 3] = a, b, w
     row = np.concatenate([base[tm] + i1, base[tm] + i2])
-    order = np.argsort(row, kind="stable")
-    inc = np.empty((len(row), 4), dtype=np.float32)
-    inc[:, 0] = np.concatenate([i2, i1])[order].astype(np.int32).view(np.float32)
-    for k, v in ((1, a), (2, b), (3, w)):
-        inc[:, k] = np.concatenate([v, v])[order]
-    return rec, _starts(np.bincount(row, minlength=rows)[:rows]), inc
+    inc, order = _incidence_rows(rec, i1, i2, row)
+    return rec, _starts(np.bincount(row, minlength=rows)[:rows]), inc, order
 
 
 def _quad_incidence(starts, quads, n_atoms, base, rows, what):
@@ -288,7 +300,7 @@ def _quad_incidence(starts, quads, n_atoms, base, rows, what):
     crow = (base[tm][:, None] + quads).reshape(-1)
     cterm = np.repeat(np.arange(len(quads), dtype=np.int64), 4)
     crole = np.tile(np.arange(4, dtype=np.int64), len(quads))
-    order = np.argsort(crow, kind="stable")
+    order = _stable_order(crow)
     inc = np.stack([cterm[order], crole[order]], axis=1).astype(np.int32) if len(crow) else np.zeros((0, 2), np.int32)
     return inc, _starts(np.bincount(crow, minlength=rows)[:rows])
 
@@ -304,41 +316,76 @@ def etk_device_arrays(batch: SharedConstraintBatch) -> dict:
         raise ValueError("the batch has no ETK terms (add_etk_to_batch)")
     n_atoms, base, rows = _atoms_and_base(batch)
     M = int(batch.n_mols)
-    fb_parts = []
-    for m in range(M):
-        for tag in ("12", "13", "14"):
-            st = np.asarray(getattr(batch, f"etk_dist{tag}_term_starts"))
-            sl = slice(int(st[m]), int(st[m + 1]))
-            fb_parts.append([np.asarray(getattr(batch, f"etk_dist{tag}_{f}"))[sl]
-                             for f in ("idx1", "idx2", "lb", "ub", "weight")])
-    fb = [np.concatenate([p[k] for p in fb_parts]) if fb_parts else np.zeros(0) for k in range(5)]
-    fb_counts = [sum(int(np.diff(np.asarray(getattr(batch, f"etk_dist{tag}_term_starts")))[m])
-                     for tag in ("12", "13", "14")) for m in range(M)]
+
+    def interleave(lists):
+        """Concatenate per-family term arrays molecule by molecule (family order kept within a
+        molecule): the permutation of the family-major concatenation, and per-molecule counts."""
+        mol = np.concatenate([_term_mol(np.asarray(st, dtype=np.int64)) for st, _ in lists]) if lists else \
+            np.zeros(0, np.int64)
+        fam = np.concatenate([np.full(len(_term_mol(np.asarray(st))), k) for k, (st, _) in enumerate(lists)])
+        order = np.lexsort((np.arange(len(mol)), fam, mol))
+        counts = np.bincount(mol, minlength=M)[:M] if len(mol) else np.zeros(M, np.int64)
+        return order, counts
+
+    fam_fb = [(getattr(batch, f"etk_dist{t}_term_starts"), t) for t in ("12", "13", "14")]
+    order, fb_counts = interleave(fam_fb)
+
+    def cat(name, dtype):
+        return np.concatenate([np.asarray(getattr(batch, f"etk_dist{t}_{name}"), dtype=dtype)
+                               for t in ("12", "13", "14")])[order]
+
     fb_starts = _starts(fb_counts)
-    fb_rec, fbinc_starts, fbinc_rec = _pair_tables(fb_starts, fb[0], fb[1], np.asarray(fb[2], np.float32),
-                                                   np.asarray(fb[3], np.float32), np.asarray(fb[4], np.float32),
-                                                   n_atoms, base, rows, "flat-bottom")
-    ts, isx = np.asarray(batch.etk_torsion_term_starts), np.asarray(batch.etk_improper_term_starts)
+    fb_src = order
+    fb_rec, fbinc_starts, fbinc_rec, inc_order = _pair_tables(fb_starts, cat("idx1", np.int64), cat("idx2", np.int64),
+                                                   cat("lb", np.float32), cat("ub", np.float32),
+                                                   cat("weight", np.float32), n_atoms, base, rows, "flat-bottom")
     tq = np.asarray(batch.etk_torsion_idx).reshape(-1, 4)
     tV = np.asarray(batch.etk_torsion_V, np.float32).reshape(-1, 6)
     tS = np.asarray(batch.etk_torsion_signs, np.float32).reshape(-1, 6)
     iq = np.asarray(batch.etk_improper_idx).reshape(-1, 4)
     iw = np.asarray(batch.etk_improper_weight, np.float32)
-    quads, coef, counts = [], [], []
-    for m in range(M):
-        t0, t1, i0, i1 = int(ts[m]), int(ts[m + 1]), int(isx[m]), int(isx[m + 1])
-        quads += [tq[t0:t1], iq[i0:i1]]
-        imp = np.zeros((i1 - i0, 12), np.float32)
-        imp[:, 1] = iw[i0:i1]
-        imp[:, 7] = -1.0
-        coef += [np.concatenate([tV[t0:t1], tS[t0:t1]], axis=1), imp]
-        counts.append((t1 - t0) + (i1 - i0))
-    tor_quads = np.concatenate(quads).astype(np.int32) if quads else np.zeros((0, 4), np.int32)
-    tor_coef = np.concatenate(coef).astype(np.float32) if coef else np.zeros((0, 12), np.float32)
+    imp = np.zeros((len(iq), 12), np.float32)
+    imp[:, 1] = iw
+    imp[:, 7] = -1.0
+    order, counts = interleave([(batch.etk_torsion_term_starts, "tor"), (batch.etk_improper_term_starts, "imp")])
+    tor_quads = np.concatenate([tq, iq]).astype(np.int32)[order].reshape(-1, 4)
+    tor_coef = np.concatenate([np.concatenate([tV, tS], axis=1), imp]).astype(np.float32)[order].reshape(-1, 12)
     tor_starts = _starts(counts)
     tinc_rec, tinc_starts = _quad_incidence(tor_starts, tor_quads, n_atoms, base, rows, "torsion")
+    # where each flat-bottom term sits, for patching its bounds in place (fb_bounds_patch):
+    # fb_row[t] is the record of term t of the 12 | 13 | 14 concatenation, and fbinc_pos[r] and
+    # fbinc_pos[r + len(fb_rec)] are record r's two incidence rows
+    fb_row = np.empty(len(fb_src), np.int64)
+    fb_row[fb_src] = np.arange(len(fb_src), dtype=np.int64)
+    fbinc_pos = np.empty(len(inc_order), np.int64)
+    fbinc_pos[inc_order] = np.arange(len(inc_order), dtype=np.int64)
     out = _conf_arrays(batch, n_atoms, base)
     out.update(fb_starts=fb_starts, fb_rec=fb_rec, fbinc_starts=fbinc_starts, fbinc_rec=fbinc_rec,
                tor_starts=tor_starts, tor_quads=tor_quads, tor_coef=tor_coef, tinc_starts=tinc_starts,
-               tinc_rec=tinc_rec, max_tor=int(max(counts)) if counts else 0)
+               tinc_rec=tinc_rec, max_tor=int(counts.max()) if len(counts) else 0,
+               fb_row=fb_row, fbinc_pos=fbinc_pos)
     return out
+
+
+def fb_bounds_patch(arrs: dict, batch: SharedConstraintBatch, tags=("12", "13")):
+    """The writes that bring ``etk_device_arrays``' flat-bottom tables up to date after the
+    bounds of the ``tags`` families changed in the batch (the pipeline's re-centred 1-2 / 1-3
+    terms; the term lists themselves unchanged): (record rows, incidence rows, (T, 2) float32
+    lb / ub).  Column 1 and 2 of ``fb_rec[rows]`` and of ``fbinc_rec[inc_rows]`` take the values,
+    the latter once per atom of a term (values repeated)."""
+    fams = ("12", "13", "14")
+    if list(tags) != list(fams[:len(tags)]):
+        raise ValueError("the patched families must lead the 12 | 13 | 14 order")
+    lb = np.concatenate([np.asarray(getattr(batch, f"etk_dist{t}_lb"), np.float32) for t in tags])
+    ub = np.concatenate([np.asarray(getattr(batch, f"etk_dist{t}_ub"), np.float32) for t in tags])
+    rows = arrs["fb_row"][:len(lb)]
+    m = len(arrs["fb_rec"])
+    inc_rows = np.concatenate([arrs["fbinc_pos"][rows], arrs["fbinc_pos"][rows + m]])
+    return rows, inc_rows, np.stack([lb, ub], axis=1)
+
+
+def patch_fb_bounds(arrs: dict, batch: SharedConstraintBatch, tags=("12", "13")) -> None:
+    """``fb_bounds_patch`` applied to the host tables (in place)."""
+    rows, inc_rows, vals = fb_bounds_patch(arrs, batch, tags)
+    arrs["fb_rec"][rows, 1:3] = vals
+    arrs["fbinc_rec"][inc_rows, 1:3] = np.concatenate([vals, vals])

@@ -232,6 +232,36 @@ def test_metric_starts_batched_equal_sequential_with_extra_draws(dg_golden):
     assert np.isfinite(got).all()
 
 
+def test_per_molecule_starts_assemble_to_the_batch_sequence(dg_golden):
+    """The pipeline computes each molecule's starts apart (its terms and its slice of the draw
+    sequence, on the process pool); assembled, they equal ``metric_matrix_positions``, also when a
+    conformer needs extra uniform columns and the rest of the batch is redone in sequence."""
+    from mlxmolkit_b200 import conformer_pipeline_v2 as cp
+    from mlxmolkit_b200.dg_extract import (embed_conformers, metric_matrix_positions, pair_draw_offsets,
+                                           uniform_draws)
+    params = _golden_synth_params(dg_golden)
+    for p, mi in zip(params, range(3)):
+        p.bounds_mat = dg_golden[f"s{mi}_bounds_mat"]
+    tiny, flat = all_pairs_dg(3), all_pairs_dg(2)
+    tiny.bounds_mat = np.array([[0, 1.5, 2.5], [1.4, 0, 1.5], [2.4, 1.4, 0]])
+    flat.bounds_mat = np.zeros((2, 2))
+    for mols, ks in ((params, [2, 3, 1]), (params + [tiny] + params[:2], [2, 1, 2, 2, 3, 1]),
+                     (params[:1] + [flat] + params[1:], [1, 2, 0, 2])):
+        b = pack_shared_dg_batch(mols, ks, dim=4)
+        offs = pair_draw_offsets(np.repeat([p.n_atoms for p in mols], ks))
+        first = np.concatenate([[0], np.cumsum(ks)])
+        res = []
+        for i, (p, k) in enumerate(zip(mols, ks)):
+            n = p.n_atoms
+            u = uniform_draws(5, int(offs[first[i]]), k * n * (n - 1) // 2)
+            res.append((p, *embed_conformers(p.bounds_mat, u, k, 4)) if k else (p, None, 0))
+        got = cp._assemble_starts(res, ks, b, 5, 4)
+        ref = metric_matrix_positions(b, [p.bounds_mat for p in mols], seed=5, dim=4)
+        assert np.array_equal(got, ref)
+        # the tiny and the zero-bounds molecule each need the extra columns at their first conformer
+        assert any(r[1] is not None and r[2] < k for r, k in zip(res, ks)) == (len(mols) > 3)
+
+
 def test_recentred_bounds_take_the_last_conformer(dg_golden):
     """conformer_pipeline_v2.py:224-258: the 1-2 / 1-3 bounds move to the measured distances of the
     molecule's last conformer, keeping their half-widths."""
@@ -262,11 +292,17 @@ def test_pooled_extraction_equals_in_process():
 
     from mlxmolkit_b200 import conformer_pipeline_v2 as cp
     from mlxmolkit_b200 import synth
+    from mlxmolkit_b200.dg_extract import metric_matrix_positions
+    from mlxmolkit_b200.shared_batch import pack_shared_dg_batch
     mols = synth.make_molecules(cp._POOL_MIN, 1, 9, 8, 16, workers=1)
     serial = [cp._dg_terms(m) for m in mols]
-    for a, b in zip(serial, cp._pmap(cp._dg_terms, mols)):
+    ks = [1 + i % 4 for i in range(len(mols))]
+    pooled, b4, x4 = cp._dg_terms_and_positions(mols, ks, 42)    # terms and starts in one task
+    for a, b in zip(serial, pooled):
         for f in fields(a):
             assert np.array_equal(np.asarray(getattr(a, f.name)), np.asarray(getattr(b, f.name))), f.name
+    ref = metric_matrix_positions(pack_shared_dg_batch(serial, ks, dim=4), [p.bounds_mat for p in serial], seed=42)
+    assert np.array_equal(x4, ref)
     items = [(m, "MMFF94s") for m in mols]
     serial = [cp._mmff_terms(x) for x in items]
     pooled = cp._pmap(cp._mmff_terms, items)

@@ -170,6 +170,24 @@ def test_device_layout_reproduces_the_oracle(dg_golden):
         np.testing.assert_allclose(g, g_ref, rtol=1e-5, atol=1e-5 * max(1.0, np.abs(g_ref).max()))
 
 
+def test_patched_bounds_equal_a_fresh_layout(dg_golden):
+    """The pipeline builds the ETK tables while the GPU runs DG and patches the re-centred 1-2 /
+    1-3 bounds in afterwards; the patched tables equal tables built from the re-centred batch."""
+    from mlxmolkit_b200.conformer_pipeline_v2 import _recenter_bounds
+    from mlxmolkit_b200.shared_batch import patch_fb_bounds
+    b = _golden_batch3(dg_golden)
+    early = etk_device_arrays(b)
+    _recenter_bounds(b, _positions(b, 12, 1.5).astype(np.float32))
+    fresh = etk_device_arrays(b)
+    assert not np.array_equal(early["fb_rec"], fresh["fb_rec"])
+    patch_fb_bounds(early, b)
+    for f in fresh:
+        if isinstance(fresh[f], np.ndarray):
+            assert np.array_equal(early[f].view(np.uint8), fresh[f].view(np.uint8)), f
+        else:
+            assert early[f] == fresh[f], f
+
+
 def test_etk_device_layout_rejects_a_4d_batch(dg_golden):
     b = _golden_batch3(dg_golden)
     b.dim = 4

@@ -101,3 +101,23 @@ def test_pipeline_stages_chain_and_agree_with_the_oracle():
     # statuses are not compared: on these stiff terms an FP32 run reaches the relative-step
     # (TOLX) exit where the FP64 run keeps descending to the budget
     assert set(np.unique(sg)) <= {0, 1}
+
+
+def test_refreshed_bounds_equal_a_fresh_upload():
+    """The pipeline uploads the ETK tables while DG runs and writes the re-centred 1-2 / 1-3
+    bounds in afterwards (ETKDeviceBatch.refresh_bounds): the device tables then equal those of
+    a batch uploaded after the re-centring."""
+    import torch
+    from mlxmolkit_b200.conformer_pipeline_v2 import _recenter_bounds
+    from mlxmolkit_b200.etk_metal import ETKDeviceBatch
+    b, _, x = _etk_batch(n_mols=5, k=2)
+    early = ETKDeviceBatch(b)
+    _recenter_bounds(b, (x + np.random.default_rng(8).normal(0, 0.2, x.shape)).astype(np.float32))
+    early.refresh_bounds()
+    fresh = ETKDeviceBatch(b)
+    torch.cuda.synchronize()
+    for f in ("fb_rec", "fbinc_rec"):
+        assert torch.equal(early.dev[f].view(torch.int32), fresh.dev[f].view(torch.int32)), f
+    eg, _ = early.energy_grad_device(torch.from_numpy(x).cuda(), early.params(0, 0.0, 0.0, 0.0))
+    ef, _ = fresh.energy_grad_device(torch.from_numpy(x).cuda(), fresh.params(0, 0.0, 0.0, 0.0))
+    assert torch.equal(eg, ef)
