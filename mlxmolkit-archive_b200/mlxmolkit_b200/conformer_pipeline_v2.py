@@ -141,9 +141,8 @@ _ONE_BLAS_THREAD = None
 def _dg_terms_and_starts(item):
     """A molecule's DG terms and the metric-matrix starts of its k conformers, from its slice of
     the batch's draw sequence (``dg_extract.embed_conformers``): (params, (k, n * dim) float32,
-    index of the first conformer that needs an extra uniform column, k when none, ETK terms or
-    None), or (params, None, 0, ETK terms or None) for a molecule the batched form does not
-    cover.  The ETK terms are extracted when ``with_etk``, from the same bounds."""
+    index of the first conformer that needs an extra uniform column, k when none), or
+    (params, None, 0) for a molecule the batched form does not cover."""
     global _ONE_BLAS_THREAD
     from .dg_extract import embed_conformers, synth_dg_params, uniform_draws
     if _ONE_BLAS_THREAD is None:                  # the pool's processes share the cores
@@ -152,38 +151,33 @@ def _dg_terms_and_starts(item):
             _ONE_BLAS_THREAD = threadpool_limits(1)
         except ImportError:
             _ONE_BLAS_THREAD = False
-    mol, k, seed, offset, dim, with_etk = item
+    mol, k, seed, offset, dim = item
     p = synth_dg_params(mol)
-    etk = _etk_terms((mol, p.bounds_mat)) if with_etk else None
     n = int(p.n_atoms)
     if p.bounds_mat is None or n <= 1 or k == 0:
-        return p, None, 0, etk
+        return p, None, 0
     xyz, j = embed_conformers(p.bounds_mat, uniform_draws(seed, offset, k * n * (n - 1) // 2), k, dim)
-    return p, xyz, j, etk
+    return p, xyz, j
 
 
-def _dg_terms_and_positions(mols, ks, seed: int, dim: int = 4, with_etk: bool = False):
-    """DG terms, the packed batch, its metric-matrix starts (``metric_matrix_positions``'s result)
-    and, when ``with_etk``, a function returning the molecules' ETK terms.  On the process pool
-    for large batches, each task one molecule's terms and starts."""
+def _dg_terms_and_positions(mols, ks, seed: int, dim: int = 4):
+    """DG terms, the packed batch and its metric-matrix starts (``metric_matrix_positions``'s
+    result); on the process pool for large batches, each task one molecule's terms and starts."""
     from .dg_extract import metric_matrix_positions, pair_draw_offsets
     from .shared_batch import pack_shared_dg_batch
     if _pool_for(len(mols)) is None:
         dgp = [_dg_terms(m) for m in mols]
         b4 = pack_shared_dg_batch(dgp, ks, dim=dim)
-        etk = (lambda: [_etk_terms((m, p.bounds_mat)) for m, p in zip(mols, dgp)]) if with_etk else None
-        return dgp, b4, metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=dim), etk
+        return dgp, b4, metric_matrix_positions(b4, [p.bounds_mat for p in dgp], seed=seed, dim=dim)
     first = np.concatenate([[0], np.cumsum(ks)]).astype(np.int64)
     offs = pair_draw_offsets(np.repeat([m.GetNumAtoms() for m in mols], ks))
-    res = _pmap(_dg_terms_and_starts, [(m, int(k), seed, int(offs[first[i]]), dim, with_etk)
+    res = _pmap(_dg_terms_and_starts, [(m, int(k), seed, int(offs[first[i]]), dim)
                                        for i, (m, k) in enumerate(zip(mols, ks))])
     dgp = [r[0] for r in res]
     b4 = pack_shared_dg_batch(dgp, ks, dim=dim)
     bounds = [p.bounds_mat for p in dgp]
     out = _assemble_starts(res, ks, b4, seed, dim)
-    etk = [r[3] for r in res]
-    return dgp, b4, out if out is not None else metric_matrix_positions(b4, bounds, seed=seed, dim=dim), \
-        (lambda: etk) if with_etk else None
+    return dgp, b4, out if out is not None else metric_matrix_positions(b4, bounds, seed=seed, dim=dim)
 
 
 def _assemble_starts(res, ks, b4, seed: int, dim: int):
@@ -198,7 +192,7 @@ def _assemble_starts(res, ks, b4, seed: int, dim: int):
     C = int(b4.n_confs_total)
     out = np.zeros(int(starts[-1]) * dim, np.float32)
     bad = C
-    for i, (_, xyz, j, _) in enumerate(res):
+    for i, (_, xyz, j) in enumerate(res):
         c0 = int(first[i])
         if xyz is None:
             continue
@@ -273,7 +267,9 @@ def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight
             timings[name] = timings.get(name, 0.0) + now - tick
             tick = now
 
-    dgp, b4, x4, etk_terms = _dg_terms_and_positions(list(mols), ks, seed, dim=4, with_etk=variant != "DG")
+    dgp, b4, x4 = _dg_terms_and_positions(list(mols), ks, seed, dim=4)
+    if variant != "DG":                          # extracted on the pool while the GPU runs DG
+        etk_terms = _pmap_async(_etk_terms, [(m, p.bounds_mat) for m, p in zip(mols, dgp)])
     background = after_host() if after_host is not None else None
     C = b4.n_confs_total
     max_atoms = max(p.n_atoms for p in dgp)

@@ -254,7 +254,7 @@ def test_per_molecule_starts_assemble_to_the_batch_sequence(dg_golden):
         for i, (p, k) in enumerate(zip(mols, ks)):
             n = p.n_atoms
             u = uniform_draws(5, int(offs[first[i]]), k * n * (n - 1) // 2)
-            res.append((p, *embed_conformers(p.bounds_mat, u, k, 4), None) if k else (p, None, 0, None))
+            res.append((p, *embed_conformers(p.bounds_mat, u, k, 4)) if k else (p, None, 0))
         got = cp._assemble_starts(res, ks, b, 5, 4)
         ref = metric_matrix_positions(b, [p.bounds_mat for p in mols], seed=5, dim=4)
         assert np.array_equal(got, ref)
@@ -297,14 +297,10 @@ def test_pooled_extraction_equals_in_process():
     mols = synth.make_molecules(cp._POOL_MIN, 1, 9, 8, 16, workers=1)
     serial = [cp._dg_terms(m) for m in mols]
     ks = [1 + i % 4 for i in range(len(mols))]
-    pooled, b4, x4, etk = cp._dg_terms_and_positions(mols, ks, 42, with_etk=True)   # one task per molecule
+    pooled, b4, x4 = cp._dg_terms_and_positions(mols, ks, 42)    # terms and starts in one task
     for a, b in zip(serial, pooled):
         for f in fields(a):
             assert np.array_equal(np.asarray(getattr(a, f.name)), np.asarray(getattr(b, f.name))), f.name
-    for m, p, e in zip(mols, serial, etk()):
-        s = cp._etk_terms((m, p.bounds_mat))
-        for f in fields(s):
-            assert np.array_equal(np.asarray(getattr(s, f.name)), np.asarray(getattr(e, f.name))), f.name
     ref = metric_matrix_positions(pack_shared_dg_batch(serial, ks, dim=4), [p.bounds_mat for p in serial], seed=42)
     assert np.array_equal(x4, ref)
     items = [(m, "MMFF94s") for m in mols]
