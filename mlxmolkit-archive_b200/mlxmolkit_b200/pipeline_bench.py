@@ -10,7 +10,10 @@ M3 Max (docs/BENCHMARKS.md:44-61).
 
 Per workload: conformers/s of the call (median of ``--repeats`` after one
 warm-up call), the fraction converged by the reference's rule (every stage),
-and the seconds of each part (embedding host / GPU, ETK host / GPU, MMFF).
+the seconds of each part (embedding host / GPU, ETK host / GPU, MMFF), and the
+host CPU: the metric-matrix starts come from LAPACK's ``eigh`` on the host,
+whose last-bit rounding can differ between CPU models, so the converged
+fraction may move by a few conformers between machines.
 
 Usage: python -m mlxmolkit_b200.pipeline_bench [--workloads 20x50,1000x10] [--repeats 3]
 """
@@ -18,12 +21,25 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
 
 import numpy as np
 
 from . import synth
 from .conformer_pipeline_v2 import generate_conformers_nk
+
+
+def _host_cpu() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def run(n_mols: int, k: int, repeats: int, seed: int = 0) -> dict:
@@ -43,7 +59,8 @@ def run(n_mols: int, k: int, repeats: int, seed: int = 0) -> dict:
     conv = np.concatenate([r.converged for r in res.molecules])
     return {"workload": f"{n_mols}x{k} synthetic, heavy atoms 10-30", "conformers": int(res.total_conformers),
             "seconds": times[i], "conf_per_s": res.total_conformers / times[i],
-            "converged": float(conv.mean()), "parts_s": {k2: round(v, 4) for k2, v in parts[i].items()}}
+            "converged": float(conv.mean()), "parts_s": {k2: round(v, 4) for k2, v in parts[i].items()},
+            "host_cpu": _host_cpu(), "host_threads": os.cpu_count()}
 
 
 def main():
