@@ -16,6 +16,8 @@ largest-first conformer order.  Host-only numpy: no device is touched here.
 """
 from __future__ import annotations
 
+import os
+
 from dataclasses import dataclass
 from typing import List, Optional
 
@@ -305,65 +307,150 @@ def _quad_incidence(starts, quads, n_atoms, base, rows, what):
     return inc, _starts(np.bincount(crow, minlength=rows)[:rows])
 
 
-def etk_device_arrays(batch: SharedConstraintBatch) -> dict:
-    """The ETK terms in the device layout of include/mmffb200_dg.h (MMFFETKTermsDev), validated.
+_FB_FAMILIES = ("12", "13", "14")
 
-    Per molecule the flat-bottom list is its 1-2, then 1-3, then 1-4 terms; the Fourier list is
-    its torsions, then its impropers as Fourier terms (V1 = w, s1 = -1, etk_metal.py:105-124)."""
-    if batch.dim != 3:
-        raise ValueError("the ETK stage is 3-D")
-    if batch.etk_torsion_term_starts is None:
-        raise ValueError("the batch has no ETK terms (add_etk_to_batch)")
-    n_atoms, base, rows = _atoms_and_base(batch)
-    M = int(batch.n_mols)
 
-    def interleave(lists):
+def _etk_view(batch: SharedConstraintBatch, m0: int, m1: int) -> dict:
+    """The ETK term arrays of molecules [m0, m1), starts relative to molecule m0."""
+    v = {"n_atoms": np.asarray(batch.mol_n_atoms, dtype=np.int64)[m0:m1]}
+
+    def part(starts_name, arrays):
+        st = np.asarray(getattr(batch, starts_name), dtype=np.int64)
+        a, b = int(st[m0]), int(st[m1])
+        return st[m0:m1 + 1] - a, [x[a:b] for x in arrays]
+
+    for t in _FB_FAMILIES:
+        names = [f"etk_dist{t}_{f}" for f in ("idx1", "idx2", "lb", "ub", "weight")]
+        v[f"st{t}"], v[f"d{t}"] = part(f"etk_dist{t}_term_starts", [np.asarray(getattr(batch, n)) for n in names])
+    v["st_tor"], (v["tq"], v["tV"], v["tS"]) = part(
+        "etk_torsion_term_starts", [np.asarray(batch.etk_torsion_idx).reshape(-1, 4),
+                                    np.asarray(batch.etk_torsion_V, np.float32).reshape(-1, 6),
+                                    np.asarray(batch.etk_torsion_signs, np.float32).reshape(-1, 6)])
+    v["st_imp"], (v["iq"], v["iw"]) = part(
+        "etk_improper_term_starts", [np.asarray(batch.etk_improper_idx).reshape(-1, 4),
+                                     np.asarray(batch.etk_improper_weight, np.float32)])
+    return v
+
+
+def _etk_tables(v: dict) -> dict:
+    """The device tables of one run of molecules (``_etk_view``), rows and terms counted from
+    the run's first molecule."""
+    n_atoms = v["n_atoms"]
+    base = np.zeros(len(n_atoms), dtype=np.int64)
+    if len(n_atoms):
+        base[1:] = np.cumsum(n_atoms)[:-1]
+    rows = int(n_atoms.sum())
+    M = len(n_atoms)
+
+    def interleave(starts_list):
         """Concatenate per-family term arrays molecule by molecule (family order kept within a
         molecule): the permutation of the family-major concatenation, and per-molecule counts."""
-        mol = np.concatenate([_term_mol(np.asarray(st, dtype=np.int64)) for st, _ in lists]) if lists else \
-            np.zeros(0, np.int64)
-        fam = np.concatenate([np.full(len(_term_mol(np.asarray(st))), k) for k, (st, _) in enumerate(lists)])
+        mol = np.concatenate([_term_mol(st) for st in starts_list])
+        fam = np.concatenate([np.full(int(st[-1]), k) for k, st in enumerate(starts_list)])
         order = np.lexsort((np.arange(len(mol)), fam, mol))
         counts = np.bincount(mol, minlength=M)[:M] if len(mol) else np.zeros(M, np.int64)
         return order, counts
 
-    fam_fb = [(getattr(batch, f"etk_dist{t}_term_starts"), t) for t in ("12", "13", "14")]
-    order, fb_counts = interleave(fam_fb)
+    order, fb_counts = interleave([v[f"st{t}"] for t in _FB_FAMILIES])
 
-    def cat(name, dtype):
-        return np.concatenate([np.asarray(getattr(batch, f"etk_dist{t}_{name}"), dtype=dtype)
-                               for t in ("12", "13", "14")])[order]
+    def cat(k, dtype):
+        return np.concatenate([np.asarray(v[f"d{t}"][k], dtype=dtype) for t in _FB_FAMILIES])[order]
 
     fb_starts = _starts(fb_counts)
-    fb_src = order
-    fb_rec, fbinc_starts, fbinc_rec, inc_order = _pair_tables(fb_starts, cat("idx1", np.int64), cat("idx2", np.int64),
-                                                   cat("lb", np.float32), cat("ub", np.float32),
-                                                   cat("weight", np.float32), n_atoms, base, rows, "flat-bottom")
-    tq = np.asarray(batch.etk_torsion_idx).reshape(-1, 4)
-    tV = np.asarray(batch.etk_torsion_V, np.float32).reshape(-1, 6)
-    tS = np.asarray(batch.etk_torsion_signs, np.float32).reshape(-1, 6)
-    iq = np.asarray(batch.etk_improper_idx).reshape(-1, 4)
-    iw = np.asarray(batch.etk_improper_weight, np.float32)
-    imp = np.zeros((len(iq), 12), np.float32)
-    imp[:, 1] = iw
+    fb_rec, fbinc_starts, fbinc_rec, inc_order = _pair_tables(
+        fb_starts, cat(0, np.int64), cat(1, np.int64), cat(2, np.float32), cat(3, np.float32),
+        cat(4, np.float32), n_atoms, base, rows, "flat-bottom")
+    imp = np.zeros((len(v["iq"]), 12), np.float32)
+    imp[:, 1] = v["iw"]
     imp[:, 7] = -1.0
-    order, counts = interleave([(batch.etk_torsion_term_starts, "tor"), (batch.etk_improper_term_starts, "imp")])
-    tor_quads = np.concatenate([tq, iq]).astype(np.int32)[order].reshape(-1, 4)
-    tor_coef = np.concatenate([np.concatenate([tV, tS], axis=1), imp]).astype(np.float32)[order].reshape(-1, 12)
+    torder, counts = interleave([v["st_tor"], v["st_imp"]])
+    tor_quads = np.concatenate([v["tq"], v["iq"]]).astype(np.int32)[torder].reshape(-1, 4)
+    tor_coef = np.concatenate([np.concatenate([v["tV"], v["tS"]], axis=1), imp]).astype(np.float32)[torder]
     tor_starts = _starts(counts)
     tinc_rec, tinc_starts = _quad_incidence(tor_starts, tor_quads, n_atoms, base, rows, "torsion")
     # where each flat-bottom term sits, for patching its bounds in place (fb_bounds_patch):
     # fb_row[t] is the record of term t of the 12 | 13 | 14 concatenation, and fbinc_pos[r] and
     # fbinc_pos[r + len(fb_rec)] are record r's two incidence rows
-    fb_row = np.empty(len(fb_src), np.int64)
-    fb_row[fb_src] = np.arange(len(fb_src), dtype=np.int64)
+    fb_row = np.empty(len(order), np.int64)
+    fb_row[order] = np.arange(len(order), dtype=np.int64)
     fbinc_pos = np.empty(len(inc_order), np.int64)
     fbinc_pos[inc_order] = np.arange(len(inc_order), dtype=np.int64)
-    out = _conf_arrays(batch, n_atoms, base)
-    out.update(fb_starts=fb_starts, fb_rec=fb_rec, fbinc_starts=fbinc_starts, fbinc_rec=fbinc_rec,
-               tor_starts=tor_starts, tor_quads=tor_quads, tor_coef=tor_coef, tinc_starts=tinc_starts,
-               tinc_rec=tinc_rec, max_tor=int(counts.max()) if len(counts) else 0,
-               fb_row=fb_row, fbinc_pos=fbinc_pos)
+    return dict(fb_starts=fb_starts, fb_rec=fb_rec, fbinc_starts=fbinc_starts, fbinc_rec=fbinc_rec,
+                tor_starts=tor_starts, tor_quads=tor_quads, tor_coef=tor_coef.reshape(-1, 12),
+                tinc_starts=tinc_starts, tinc_rec=tinc_rec, max_tor=int(counts.max()) if len(counts) else 0,
+                fb_row=fb_row, fbinc_pos=fbinc_pos,
+                fam_sizes=[int(v[f"st{t}"][-1]) for t in _FB_FAMILIES])
+
+
+def _etk_runs(batch: SharedConstraintBatch, parts: int):
+    """Contiguous runs of molecules with about equal numbers of flat-bottom terms."""
+    M = int(batch.n_mols)
+    per_mol = sum(np.diff(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"), dtype=np.int64))
+                  for t in _FB_FAMILIES)
+    cuts = np.searchsorted(np.cumsum(per_mol), np.arange(1, parts) * (per_mol.sum() / parts), side="right")
+    bounds = np.unique(np.concatenate([[0], np.clip(cuts, 1, M - 1), [M]])) if M > 1 else np.array([0, M])
+    return [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
+
+
+def _merge_etk(parts, runs, batch) -> dict:
+    """One batch's tables from its runs' tables: records concatenate, starts re-accumulate, and
+    the term and record indices the runs counted locally move to the batch's numbering."""
+    cat = lambda k: np.concatenate([p[k] for p in parts])
+    counts = lambda k: np.concatenate([np.diff(p[k]) for p in parts])
+    fb_starts, tor_starts = _starts(counts("fb_starts")), _starts(counts("tor_starts"))
+    tinc = []
+    for p, (m0, _) in zip(parts, runs):
+        t = p["tinc_rec"].copy()
+        t[:, 0] += tor_starts[m0]
+        tinc.append(t)
+    total = sum(len(p["fb_row"]) for p in parts)
+    fb_row = np.empty(total, np.int64)
+    fbinc_pos = np.empty(2 * total, np.int64)
+    fam_off = np.concatenate([[0], np.cumsum([int(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"))[-1])
+                                              for t in _FB_FAMILIES])])
+    for p, (m0, _) in zip(parts, runs):
+        rec0, mc = int(fb_starts[m0]), len(p["fb_rec"])
+        local = 0
+        for f, t in enumerate(_FB_FAMILIES):
+            g0 = int(fam_off[f]) + int(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"))[m0])
+            n = p["fam_sizes"][f]
+            fb_row[g0:g0 + n] = p["fb_row"][local:local + n] + rec0
+            local += n
+        fbinc_pos[rec0:rec0 + mc] = p["fbinc_pos"][:mc] + 2 * rec0
+        fbinc_pos[total + rec0:total + rec0 + mc] = p["fbinc_pos"][mc:] + 2 * rec0
+    return dict(fb_starts=fb_starts, fb_rec=cat("fb_rec"), fbinc_starts=_starts(counts("fbinc_starts")),
+                fbinc_rec=cat("fbinc_rec"), tor_starts=tor_starts, tor_quads=cat("tor_quads"),
+                tor_coef=cat("tor_coef"), tinc_starts=_starts(counts("tinc_starts")),
+                tinc_rec=np.concatenate(tinc) if tinc else np.zeros((0, 2), np.int32),
+                max_tor=max(p["max_tor"] for p in parts), fb_row=fb_row, fbinc_pos=fbinc_pos)
+
+
+def etk_device_arrays(batch: SharedConstraintBatch, workers: Optional[int] = None) -> dict:
+    """The ETK terms in the device layout of include/mmffb200_dg.h (MMFFETKTermsDev), validated.
+
+    Per molecule the flat-bottom list is its 1-2, then 1-3, then 1-4 terms; the Fourier list is
+    its torsions, then its impropers as Fourier terms (V1 = w, s1 = -1, etk_metal.py:105-124).
+    Large batches are built as runs of molecules on host threads (``workers``, default up to 16)
+    and merged; the result does not depend on the split."""
+    if batch.dim != 3:
+        raise ValueError("the ETK stage is 3-D")
+    if batch.etk_torsion_term_starts is None:
+        raise ValueError("the batch has no ETK terms (add_etk_to_batch)")
+    n_atoms, base, _ = _atoms_and_base(batch)
+    M = int(batch.n_mols)
+    n_fb = sum(int(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"))[-1]) for t in _FB_FAMILIES)
+    if workers is None:
+        workers = min(16, os.cpu_count() or 1, max(1, n_fb // 65536))
+    runs = _etk_runs(batch, max(1, min(int(workers), M))) if M else [(0, 0)]
+    if len(runs) == 1:
+        out = _etk_tables(_etk_view(batch, *runs[0]))
+        del out["fam_sizes"]
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(len(runs)) as ex:
+            parts = list(ex.map(lambda r: _etk_tables(_etk_view(batch, *r)), runs))
+        out = _merge_etk(parts, runs, batch)
+    out.update(_conf_arrays(batch, n_atoms, base))
     return out
 
 

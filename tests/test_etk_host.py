@@ -10,8 +10,8 @@
 import numpy as np
 import pytest
 
-from helpers import dg_golden_mol
-from mlxmolkit_b200.dg_extract import DGParams, synth_bounds_matrix
+from helpers import all_pairs_dg, dg_golden_mol
+from mlxmolkit_b200.dg_extract import DGParams, synth_bounds_matrix, synth_dg_params
 from mlxmolkit_b200.etk_extract import ETKParams, synth_etk_params
 from mlxmolkit_b200.shared_batch import add_etk_to_batch, etk_device_arrays, pack_shared_dg_batch
 from oracle import dg
@@ -186,6 +186,47 @@ def test_patched_bounds_equal_a_fresh_layout(dg_golden):
             assert np.array_equal(early[f].view(np.uint8), fresh[f].view(np.uint8)), f
         else:
             assert early[f] == fresh[f], f
+
+
+def _empty_etk(n):
+    z4, z6 = np.zeros((0, 4), np.int32), np.zeros((0, 6), np.float32)
+    e, i = np.zeros(0, np.float32), np.zeros(0, np.int32)
+    return ETKParams(n, z4, z6, np.zeros((0, 6), np.int32), z4, e, *([i, i, e, e, e] * 3))
+
+
+def test_etk_layout_does_not_depend_on_the_thread_split(dg_golden):
+    """Large batches build their tables as runs of molecules on host threads and merge them;
+    every split gives the bytes of the one-run build, patch indices included."""
+    from mlxmolkit_b200 import synth
+    g = dg_golden
+    dgp = [DGParams(n_atoms=len(g[f"s{mi}_elements"]), **{f: g[f"s{mi}_ref_{f}"] for f in PARAM_FIELDS})
+           for mi in range(3)]
+    etk = [ETKParams(n_atoms=len(g[f"s{mi}_elements"]), **{f: g[f"s{mi}_etk_{f}"] for f in ETK_FIELDS})
+           for mi in range(3)]
+    dist_b, _ = _distance_only_batch()
+    mols = synth.make_molecules(20, 1, 13, 6, 14, workers=1)
+    sp = [synth_dg_params(m) for m in mols]
+    dgp = dgp[:2] + [all_pairs_dg(3), all_pairs_dg(4)] + dgp[2:] + sp
+    etk = etk[:2] + [_one_etk(dist_b), _empty_etk(4)] + etk[2:] + [synth_etk_params(m, p.bounds_mat)
+                                                                   for m, p in zip(mols, sp)]
+    b = pack_shared_dg_batch(dgp, [1 + i % 3 for i in range(len(dgp))], dim=3)
+    add_etk_to_batch(b, etk)
+    one = etk_device_arrays(b, workers=1)
+    from mlxmolkit_b200.shared_batch import _etk_runs
+    for w in (2, 3, 5, 7):
+        assert len(_etk_runs(b, w)) > 1
+        got = etk_device_arrays(b, workers=w)
+        assert set(got) == set(one)
+        for f in one:
+            if isinstance(one[f], np.ndarray):
+                assert got[f].dtype == one[f].dtype and np.array_equal(got[f].view(np.uint8), one[f].view(np.uint8)), (w, f)
+            else:
+                assert got[f] == one[f], (w, f)
+
+
+def _one_etk(b):
+    """The ETKParams of a one-molecule batch's etk_* fields."""
+    return ETKParams(int(b.mol_n_atoms[0]), *[np.asarray(getattr(b, "etk_" + f)) for f in ETK_FIELDS])
 
 
 def test_etk_device_layout_rejects_a_4d_batch(dg_golden):
