@@ -74,12 +74,6 @@ def synth_etk_params(mol, bounds_mat: np.ndarray) -> ETKParams:
     ring_of = list(getattr(mol, "ring_of", [-1] * n))
     arom = np.asarray(getattr(mol, "aromatic", np.zeros(n, bool)), dtype=bool)
 
-    def ub(i, j):
-        return bm[min(i, j), max(i, j)]
-
-    def lb(i, j):
-        return bm[max(i, j), min(i, j)]
-
     tq, tv, ts = [], [], []
     seen_ring = set()
     for bd in mol.GetBonds():
@@ -122,58 +116,53 @@ def synth_etk_params(mol, bounds_mat: np.ndarray) -> ETKParams:
         for p in ((n0, n1, n2), (n1, n2, n0), (n2, n0, n1)):
             iq.append([c0, *p]), iw.append(w)
 
-    d12 = [(min(i, j), max(i, j)) for i, j in ((bd.GetBeginAtomIdx(), bd.GetEndAtomIdx()) for bd in mol.GetBonds())]
-    d12 = [(i, j) for i, j in d12 if ub(i, j) > 0 and lb(i, j) > 0]
-    d13 = []
-    for c0 in range(n):
-        nb = sorted(nbrs[c0])
-        for x in range(len(nb)):
-            for y in range(x + 1, len(nb)):
-                i, j = nb[x], nb[y]
-                if ub(i, j) > 0 and lb(i, j) > 0:
-                    d13.append((i, j))
-    d14, seen = [], set()
-    for bd in mol.GetBonds():
-        b, c = bd.GetBeginAtomIdx(), bd.GetEndAtomIdx()
-        for a in nbrs[b]:
-            if a == c:
-                continue
-            for d in nbrs[c]:
-                if d in (a, b) or a >= d:
-                    continue
-                if ub(a, d) > 0 and lb(a, d) > 0 and (a, d) not in seen:
-                    seen.add((a, d))
-                    d14.append((a, d, lb(a, d), ub(a, d), DIST14_WEIGHT))
+    def pairs(cand):
+        """(i, j) arrays of the candidate pairs whose bounds are both positive, order kept."""
+        c = np.asarray(cand, dtype=np.int64).reshape(-1, 2)
+        keep = (bm[c[:, 0], c[:, 1]] > 0) & (bm[c[:, 1], c[:, 0]] > 0) if len(c) else np.zeros(0, bool)
+        return c[keep, 0], c[keep, 1]
+
+    bonds = [(bd.GetBeginAtomIdx(), bd.GetEndAtomIdx()) for bd in mol.GetBonds()]
+    i12, j12 = pairs([(min(i, j), max(i, j)) for i, j in bonds])
+    i13, j13 = pairs([(nb[x], nb[y]) for nb in (sorted(v) for v in nbrs)
+                      for x in range(len(nb)) for y in range(x + 1, len(nb))])
+    # 1-4 pairs (a < d) through each bond b-c, first occurrence kept
+    a14, d14 = pairs([(a, d) for b, c in bonds for a in nbrs[b] if a != c for d in nbrs[c] if d != b and a < d])
+    if len(a14):
+        _, first = np.unique(a14 * n + d14, return_index=True)
+        first.sort()
+        a14, d14 = a14[first], d14[first]
     topo = np.asarray(mol.distance_matrix())
     iu, ju = np.triu_indices(n, 1)                 # row-major, as the reference's double loop
     keep = (topo[iu, ju] >= 4) & (bm[iu, ju] > 0) & (bm[ju, iu] > 0)
-    if seen:
+    if len(a14):
         taken = np.zeros((n, n), dtype=bool)
-        taken[tuple(np.array(sorted(seen)).T)] = True
+        taken[a14, d14] = True
         keep &= ~taken[iu, ju]
-    for a, d in zip(iu[keep].tolist(), ju[keep].tolist()):
-        d14.append((a, d, bm[d, a], bm[a, d], LONG_RANGE_WEIGHT))
+    iL, jL = iu[keep], ju[keep]
+    i14, j14 = np.concatenate([a14, iL]), np.concatenate([d14, jL])
+    w14 = np.concatenate([np.full(len(a14), DIST14_WEIGHT), np.full(len(iL), LONG_RANGE_WEIGHT)])
 
     def mid(i, j):
-        return 0.5 * (lb(i, j) + ub(i, j))
+        return 0.5 * (bm[j, i] + bm[i, j])
 
     def i32(x, shape=(0,)):
-        return np.array(x, dtype=np.int32).reshape(-1, *shape[1:]) if x else np.zeros(shape, np.int32)
+        return np.array(x, dtype=np.int32).reshape(-1, *shape[1:]) if len(x) else np.zeros(shape, np.int32)
 
     def f32(x, shape=(0,)):
-        return np.array(x, dtype=np.float32).reshape(-1, *shape[1:]) if x else np.zeros(shape, np.float32)
+        return np.array(x, dtype=np.float32).reshape(-1, *shape[1:]) if len(x) else np.zeros(shape, np.float32)
 
     return ETKParams(
         n_atoms=n,
         torsion_idx=i32(tq, (0, 4)), torsion_V=f32(tv, (0, 6)), torsion_signs=i32(ts, (0, 6)),
         improper_idx=i32(iq, (0, 4)), improper_weight=f32(iw),
-        dist12_idx1=i32([i for i, _ in d12]), dist12_idx2=i32([j for _, j in d12]),
-        dist12_lb=f32([mid(i, j) - BOND_TOL for i, j in d12]), dist12_ub=f32([mid(i, j) + BOND_TOL for i, j in d12]),
-        dist12_weight=f32([BOND_FC] * len(d12)),
-        dist13_idx1=i32([i for i, _ in d13]), dist13_idx2=i32([j for _, j in d13]),
-        dist13_lb=f32([mid(i, j) - BOND_TOL for i, j in d13]), dist13_ub=f32([mid(i, j) + BOND_TOL for i, j in d13]),
-        dist13_weight=f32([ANGLE_FC] * len(d13)),
-        dist14_idx1=i32([t[0] for t in d14]), dist14_idx2=i32([t[1] for t in d14]),
-        dist14_lb=f32([t[2] for t in d14]), dist14_ub=f32([t[3] for t in d14]),
-        dist14_weight=f32([t[4] for t in d14]),
+        dist12_idx1=i32(i12), dist12_idx2=i32(j12),
+        dist12_lb=f32(mid(i12, j12) - BOND_TOL), dist12_ub=f32(mid(i12, j12) + BOND_TOL),
+        dist12_weight=f32(np.full(len(i12), BOND_FC)),
+        dist13_idx1=i32(i13), dist13_idx2=i32(j13),
+        dist13_lb=f32(mid(i13, j13) - BOND_TOL), dist13_ub=f32(mid(i13, j13) + BOND_TOL),
+        dist13_weight=f32(np.full(len(i13), ANGLE_FC)),
+        dist14_idx1=i32(i14), dist14_idx2=i32(j14),
+        dist14_lb=f32(bm[j14, i14]), dist14_ub=f32(bm[i14, j14]),
+        dist14_weight=f32(w14),
     )
