@@ -167,44 +167,54 @@ def _incidence_rows(rec: np.ndarray, i1: np.ndarray, i2: np.ndarray, row: np.nda
     return both[order], order
 
 
-def dg_device_arrays(batch: SharedConstraintBatch) -> dict:
-    """The device layout of include/mmffb200_dg.h as numpy arrays (validated)."""
-    if batch.dim not in (3, 4):
-        raise ValueError(f"dim must be 3 or 4, got {batch.dim}")
-    n_atoms = np.asarray(batch.mol_n_atoms, dtype=np.int64)
-    if len(n_atoms) and (n_atoms.min() < 1 or n_atoms.max() > 1024):
-        raise ValueError("molecules must have 1..1024 atoms")
+def _dg_view(batch: SharedConstraintBatch, m0: int, m1: int) -> dict:
+    """The DG term arrays of molecules [m0, m1), starts relative to molecule m0."""
+    v = {"n_atoms": np.asarray(batch.mol_n_atoms, dtype=np.int64)[m0:m1]}
+
+    def part(starts_name, names):
+        st = np.asarray(getattr(batch, starts_name), dtype=np.int64)
+        a, b = int(st[m0]), int(st[m1])
+        return st[m0:m1 + 1] - a, [np.asarray(getattr(batch, nm))[a:b] for nm in names]
+
+    v["ds"], v["dist"] = part("dist_term_starts", ("dist_idx1", "dist_idx2", "dist_lb2", "dist_ub2", "dist_weight"))
+    v["cs"], v["chiral"] = part("chiral_term_starts", ("chiral_idx1", "chiral_idx2", "chiral_idx3", "chiral_idx4",
+                                                       "chiral_vol_lower", "chiral_vol_upper"))
+    v["fs"], (v["fi"],) = part("fourth_term_starts", ("fourth_idx",))
+    return v
+
+
+def _dg_tables(v: dict) -> dict:
+    """The DG device tables of one run of molecules (``_dg_view``), rows and terms counted from
+    the run's first molecule."""
+    n_atoms = v["n_atoms"]
     base = np.zeros(len(n_atoms), dtype=np.int64)
     if len(n_atoms):
         base[1:] = np.cumsum(n_atoms)[:-1]
     rows = int(n_atoms.sum())
 
-    ds = np.asarray(batch.dist_term_starts, dtype=np.int64)
+    ds = v["ds"]
     dm = _term_mol(ds)
-    i1 = np.asarray(batch.dist_idx1, dtype=np.int64)
-    i2 = np.asarray(batch.dist_idx2, dtype=np.int64)
+    i1 = np.asarray(v["dist"][0], dtype=np.int64)
+    i2 = np.asarray(v["dist"][1], dtype=np.int64)
     if len(i1) and (min(i1.min(), i2.min()) < 0 or np.any(i1 >= n_atoms[dm]) or np.any(i2 >= n_atoms[dm])):
         raise ValueError("distance term atom index out of range for its molecule")
-    lb2 = np.asarray(batch.dist_lb2, dtype=np.float32)
-    ub2 = np.asarray(batch.dist_ub2, dtype=np.float32)
-    w = np.asarray(batch.dist_weight, dtype=np.float32)
     dist_rec = np.empty((len(i1), 4), dtype=np.float32)
     dist_rec[:, 0] = (i1 | (i2 << 16)).astype(np.int32).view(np.float32)
-    dist_rec[:, 1], dist_rec[:, 2], dist_rec[:, 3] = lb2, ub2, w
+    for k in (1, 2, 3):
+        dist_rec[:, k] = np.asarray(v["dist"][k + 1], dtype=np.float32)
     # every distance term under both of its atoms, term order kept within a row
     row = np.concatenate([base[dm] + i1, base[dm] + i2])
     dinc_rec, _ = _incidence_rows(dist_rec, i1, i2, row)
     dinc_starts = _starts(np.bincount(row, minlength=rows)[:rows])
 
-    cs = np.asarray(batch.chiral_term_starts, dtype=np.int64)
+    cs = v["cs"]
     cm = _term_mol(cs)
-    quads = np.stack([np.asarray(getattr(batch, f"chiral_idx{k}"), dtype=np.int64) for k in (1, 2, 3, 4)], axis=1) \
+    quads = np.stack([np.asarray(v["chiral"][k], dtype=np.int64) for k in range(4)], axis=1) \
         if len(cm) else np.zeros((0, 4), np.int64)
     if len(quads) and (quads.min() < 0 or np.any(quads >= n_atoms[cm][:, None])):
         raise ValueError("chiral term atom index out of range for its molecule")
-    chiral_bounds = np.stack([np.asarray(batch.chiral_vol_lower, np.float32),
-                              np.asarray(batch.chiral_vol_upper, np.float32)], axis=1) \
-        if len(cm) else np.zeros((0, 2), np.float32)
+    chiral_bounds = np.stack([np.asarray(v["chiral"][4], np.float32), np.asarray(v["chiral"][5], np.float32)],
+                             axis=1) if len(cm) else np.zeros((0, 2), np.float32)
     crow = (base[cm][:, None] + quads).reshape(-1)
     cterm = np.repeat(np.arange(len(quads), dtype=np.int64), 4)
     crole = np.tile(np.arange(4, dtype=np.int64), len(quads))
@@ -213,24 +223,69 @@ def dg_device_arrays(batch: SharedConstraintBatch) -> dict:
         else np.zeros((0, 2), np.int32)
     cinc_starts = _starts(np.bincount(crow, minlength=rows)[:rows])
 
-    fs = np.asarray(batch.fourth_term_starts, dtype=np.int64)
-    fm = _term_mol(fs)
-    fi = np.asarray(batch.fourth_idx, dtype=np.int64)
+    fm = _term_mol(v["fs"])
+    fi = np.asarray(v["fi"], dtype=np.int64)
     if len(fi) and (fi.min() < 0 or np.any(fi >= n_atoms[fm])):
         raise ValueError("fourth-dimension atom index out of range for its molecule")
     fourth_count = np.bincount(base[fm] + fi, minlength=rows)[:rows].astype(np.int32)
+    return dict(dist_starts=ds.astype(np.int32), dist_rec=dist_rec, dinc_starts=dinc_starts, dinc_rec=dinc_rec,
+                chiral_starts=cs.astype(np.int32), chiral_quads=quads.astype(np.int32),
+                chiral_bounds=chiral_bounds.astype(np.float32), cinc_starts=cinc_starts, cinc_rec=cinc_rec,
+                fourth_count=fourth_count)
 
-    conf_to_mol = np.asarray(batch.conf_to_mol, dtype=np.int32)
-    conf_order = np.argsort(-n_atoms[conf_to_mol], kind="stable").astype(np.int32) if len(conf_to_mol) \
-        else np.zeros(0, np.int32)
-    return dict(
-        conf_to_mol=conf_to_mol, conf_atom_starts=np.asarray(batch.conf_atom_starts, dtype=np.int32),
-        conf_order=conf_order, mol_n_atoms=n_atoms.astype(np.int32), mol_atom_base=base.astype(np.int32),
-        dist_starts=ds.astype(np.int32), dist_rec=dist_rec, dinc_starts=dinc_starts, dinc_rec=dinc_rec,
-        chiral_starts=cs.astype(np.int32), chiral_quads=quads.astype(np.int32),
-        chiral_bounds=chiral_bounds.astype(np.float32), cinc_starts=cinc_starts, cinc_rec=cinc_rec,
-        fourth_count=fourth_count, max_atoms=int(n_atoms.max()) if len(n_atoms) else 1,
-    )
+
+def _runs_by_terms(per_mol: np.ndarray, parts: int):
+    """Contiguous runs of molecules with about equal numbers of terms (``per_mol`` per molecule)."""
+    M = len(per_mol)
+    cuts = np.searchsorted(np.cumsum(per_mol), np.arange(1, parts) * (per_mol.sum() / parts), side="right")
+    bounds = np.unique(np.concatenate([[0], np.clip(cuts, 1, M - 1), [M]])) if M > 1 else np.array([0, M])
+    return [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
+
+
+def _map_runs(fn, runs):
+    """``fn`` over the runs, on host threads when there is more than one (numpy releases the
+    interpreter lock in the large sorts and gathers)."""
+    if len(runs) == 1:
+        return [fn(runs[0])]
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(runs)) as ex:
+        return list(ex.map(fn, runs))
+
+
+def _default_workers(n_terms: int) -> int:
+    return min(16, os.cpu_count() or 1, max(1, n_terms // 65536))
+
+
+def dg_device_arrays(batch: SharedConstraintBatch, workers: Optional[int] = None) -> dict:
+    """The device layout of include/mmffb200_dg.h as numpy arrays (validated).  Large batches
+    are built as runs of molecules on host threads (``workers``, default up to 16) and merged;
+    the result does not depend on the split."""
+    if batch.dim not in (3, 4):
+        raise ValueError(f"dim must be 3 or 4, got {batch.dim}")
+    n_atoms, base, _ = _atoms_and_base(batch)
+    M = len(n_atoms)
+    ds = np.asarray(batch.dist_term_starts, dtype=np.int64)
+    w = _default_workers(int(ds[-1])) if workers is None else int(workers)
+    runs = _runs_by_terms(np.diff(ds), max(1, min(w, M))) if M else [(0, 0)]
+    parts = _map_runs(lambda r: _dg_tables(_dg_view(batch, *r)), runs)
+    if len(parts) == 1:
+        out = parts[0]
+    else:
+        cat = lambda k: np.concatenate([p[k] for p in parts])
+        counts = lambda k: np.concatenate([np.diff(p[k]) for p in parts])
+        chiral_starts = _starts(counts("chiral_starts"))
+        cinc = []
+        for p, (m0, _) in zip(parts, runs):
+            c = p["cinc_rec"].copy()
+            c[:, 0] += chiral_starts[m0]
+            cinc.append(c)
+        out = dict(dist_starts=_starts(counts("dist_starts")), dist_rec=cat("dist_rec"),
+                   dinc_starts=_starts(counts("dinc_starts")), dinc_rec=cat("dinc_rec"),
+                   chiral_starts=chiral_starts, chiral_quads=cat("chiral_quads"),
+                   chiral_bounds=cat("chiral_bounds"), cinc_starts=_starts(counts("cinc_starts")),
+                   cinc_rec=np.concatenate(cinc), fourth_count=cat("fourth_count"))
+    out.update(_conf_arrays(batch, n_atoms, base))
+    return out
 
 
 def add_etk_to_batch(batch: SharedConstraintBatch, etk_params_list: List[ETKParams]) -> None:
@@ -384,12 +439,8 @@ def _etk_tables(v: dict) -> dict:
 
 def _etk_runs(batch: SharedConstraintBatch, parts: int):
     """Contiguous runs of molecules with about equal numbers of flat-bottom terms."""
-    M = int(batch.n_mols)
-    per_mol = sum(np.diff(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"), dtype=np.int64))
-                  for t in _FB_FAMILIES)
-    cuts = np.searchsorted(np.cumsum(per_mol), np.arange(1, parts) * (per_mol.sum() / parts), side="right")
-    bounds = np.unique(np.concatenate([[0], np.clip(cuts, 1, M - 1), [M]])) if M > 1 else np.array([0, M])
-    return [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
+    return _runs_by_terms(sum(np.diff(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"), dtype=np.int64))
+                              for t in _FB_FAMILIES), parts)
 
 
 def _merge_etk(parts, runs, batch) -> dict:
@@ -439,16 +490,13 @@ def etk_device_arrays(batch: SharedConstraintBatch, workers: Optional[int] = Non
     n_atoms, base, _ = _atoms_and_base(batch)
     M = int(batch.n_mols)
     n_fb = sum(int(np.asarray(getattr(batch, f"etk_dist{t}_term_starts"))[-1]) for t in _FB_FAMILIES)
-    if workers is None:
-        workers = min(16, os.cpu_count() or 1, max(1, n_fb // 65536))
-    runs = _etk_runs(batch, max(1, min(int(workers), M))) if M else [(0, 0)]
-    if len(runs) == 1:
-        out = _etk_tables(_etk_view(batch, *runs[0]))
+    w = _default_workers(n_fb) if workers is None else int(workers)
+    runs = _etk_runs(batch, max(1, min(w, M))) if M else [(0, 0)]
+    parts = _map_runs(lambda r: _etk_tables(_etk_view(batch, *r)), runs)
+    if len(parts) == 1:
+        out = parts[0]
         del out["fam_sizes"]
     else:
-        from concurrent.futures import ThreadPoolExecutor
-        with ThreadPoolExecutor(len(runs)) as ex:
-            parts = list(ex.map(lambda r: _etk_tables(_etk_view(batch, *r)), runs))
         out = _merge_etk(parts, runs, batch)
     out.update(_conf_arrays(batch, n_atoms, base))
     return out

@@ -262,6 +262,28 @@ def test_per_molecule_starts_assemble_to_the_batch_sequence(dg_golden):
         assert any(r[1] is not None and r[2] < k for r, k in zip(res, ks)) == (len(mols) > 3)
 
 
+def test_dg_layout_does_not_depend_on_the_thread_split(dg_golden):
+    """Large batches build the DG tables as runs of molecules on host threads and merge them;
+    every split gives the bytes of the one-run build (distance, chiral and fourth-dimension
+    terms, molecules without chiral terms included)."""
+    from mlxmolkit_b200.shared_batch import _runs_by_terms
+    params = _golden_synth_params(dg_golden) + dg_synth_params(12, 21) + [all_pairs_dg(3), all_pairs_dg(5)]
+    ks = [1 + i % 3 for i in range(len(params))]
+    for dim in (4, 3):
+        b = pack_shared_dg_batch(params, ks, dim=dim)
+        one = dg_device_arrays(b, workers=1)
+        for w in (2, 3, 6):
+            assert len(_runs_by_terms(np.diff(np.asarray(b.dist_term_starts)), w)) > 1
+            got = dg_device_arrays(b, workers=w)
+            assert set(got) == set(one)
+            for f in one:
+                if isinstance(one[f], np.ndarray):
+                    assert got[f].dtype == one[f].dtype and np.array_equal(got[f].view(np.uint8),
+                                                                            one[f].view(np.uint8)), (dim, w, f)
+                else:
+                    assert got[f] == one[f], (dim, w, f)
+
+
 def test_recentred_bounds_take_the_last_conformer(dg_golden):
     """conformer_pipeline_v2.py:224-258: the 1-2 / 1-3 bounds move to the measured distances of the
     molecule's last conformer, keeping their half-widths."""
