@@ -226,24 +226,26 @@ def _mmff_terms(mol_and_variant):
 def _recenter_bounds(b3, pos3: np.ndarray) -> None:
     """Re-centre each molecule's 1-2 / 1-3 ETK bounds on the measured 3-D distances, keeping
     their half-widths (conformer_pipeline_v2.py:224-258; the last conformer of a molecule wins)."""
-    last = {}
-    for c in range(b3.n_confs_total):
-        last[int(b3.conf_to_mol[c])] = c
+    C = int(b3.n_confs_total)
+    conf_mol = np.asarray(b3.conf_to_mol, dtype=np.int64)[:C]
+    last = np.full(int(b3.n_mols), -1, np.int64)
+    last[conf_mol] = np.arange(C, dtype=np.int64)             # the last write of a molecule wins
+    first_atom = np.asarray(b3.conf_atom_starts, dtype=np.int64)[np.maximum(last, 0)]
+    X = np.asarray(pos3).reshape(-1, 3).astype(np.float64)
     for tag in ("12", "13"):
-        st = getattr(b3, f"etk_dist{tag}_term_starts")
-        i1, i2 = getattr(b3, f"etk_dist{tag}_idx1"), getattr(b3, f"etk_dist{tag}_idx2")
+        st = np.asarray(getattr(b3, f"etk_dist{tag}_term_starts"), dtype=np.int64)
+        tm = np.repeat(np.arange(len(st) - 1, dtype=np.int64), np.diff(st))
+        sel = np.nonzero(last[tm] >= 0)[0]                    # molecules with a conformer
+        if len(sel) == 0:
+            continue
+        i1 = np.asarray(getattr(b3, f"etk_dist{tag}_idx1"), dtype=np.int64)[sel]
+        i2 = np.asarray(getattr(b3, f"etk_dist{tag}_idx2"), dtype=np.int64)[sel]
         lb, ub = getattr(b3, f"etk_dist{tag}_lb"), getattr(b3, f"etk_dist{tag}_ub")
-        for m, c in last.items():
-            t0, t1 = int(st[m]), int(st[m + 1])
-            if t1 == t0:
-                continue
-            n = int(b3.mol_n_atoms[m])
-            a0 = int(b3.conf_atom_starts[c]) * 3
-            x = pos3[a0:a0 + 3 * n].reshape(n, 3).astype(np.float64)
-            d = np.linalg.norm(x[i1[t0:t1]] - x[i2[t0:t1]], axis=1)
-            hw = (ub[t0:t1].astype(np.float64) - lb[t0:t1]) / 2.0
-            lb[t0:t1] = (d - hw).astype(np.float32)
-            ub[t0:t1] = (d + hw).astype(np.float32)
+        a0 = first_atom[tm[sel]]
+        d = np.linalg.norm(X[a0 + i1] - X[a0 + i2], axis=1)
+        hw = (ub[sel].astype(np.float64) - lb[sel]) / 2.0
+        lb[sel] = (d - hw).astype(np.float32)
+        ub[sel] = (d + hw).astype(np.float32)
 
 
 def _embed_on_device(mols, ks, *, dg_max_iters, etk_max_iters, fourth_dim_weight, chiral_weight, variant,
