@@ -307,6 +307,41 @@ def test_recentred_bounds_take_the_last_conformer(dg_golden):
         np.testing.assert_allclose(b3.etk_dist12_ub[t0:t1], d + hw[t0:t1], atol=1e-5)
 
 
+def test_recentring_is_the_per_molecule_computation_bit_for_bit(dg_golden):
+    """The vectorised re-centring gives the bytes of the reference's per-molecule loop: FP64
+    distances of the molecule's last conformer, FP64 half-widths, rounded once to FP32; a
+    molecule without conformers keeps its bounds."""
+    from mlxmolkit_b200.conformer_pipeline_v2 import _recenter_bounds
+    from mlxmolkit_b200.etk_extract import synth_etk_params
+    from mlxmolkit_b200.shared_batch import add_etk_to_batch
+    params = _golden_synth_params(dg_golden)
+    mols = [dg_golden_mol(dg_golden, mi) for mi in range(3)]
+    ks = [3, 0, 2]
+    b3 = pack_shared_dg_batch(params, ks, dim=3)
+    add_etk_to_batch(b3, [synth_etk_params(m, dg_golden[f"s{mi}_bounds_mat"]) for mi, m in enumerate(mols)])
+    pos = np.random.default_rng(4).normal(0, 2.0, int(b3.conf_atom_starts[-1]) * 3).astype(np.float32)
+    want = {}
+    for tag in ("12", "13"):
+        st = getattr(b3, f"etk_dist{tag}_term_starts")
+        lb = getattr(b3, f"etk_dist{tag}_lb").copy()
+        ub = getattr(b3, f"etk_dist{tag}_ub").copy()
+        for m, last in ((0, 2), (2, 4)):
+            t0, t1 = int(st[m]), int(st[m + 1])
+            n, a0 = int(b3.mol_n_atoms[m]), int(b3.conf_atom_starts[last]) * 3
+            x = pos[a0:a0 + 3 * n].reshape(n, 3).astype(np.float64)
+            i1, i2 = getattr(b3, f"etk_dist{tag}_idx1")[t0:t1], getattr(b3, f"etk_dist{tag}_idx2")[t0:t1]
+            d = np.linalg.norm(x[i1] - x[i2], axis=1)
+            hw = (ub[t0:t1].astype(np.float64) - lb[t0:t1]) / 2.0
+            lb[t0:t1], ub[t0:t1] = (d - hw).astype(np.float32), (d + hw).astype(np.float32)
+        want[tag] = lb, ub
+    before13 = b3.etk_dist13_lb[b3.etk_dist13_term_starts[1]:b3.etk_dist13_term_starts[2]].copy()
+    _recenter_bounds(b3, pos)
+    for tag, (lb, ub) in want.items():
+        assert np.array_equal(getattr(b3, f"etk_dist{tag}_lb").view(np.uint32), lb.view(np.uint32)), tag
+        assert np.array_equal(getattr(b3, f"etk_dist{tag}_ub").view(np.uint32), ub.view(np.uint32)), tag
+    assert np.array_equal(b3.etk_dist13_lb[b3.etk_dist13_term_starts[1]:b3.etk_dist13_term_starts[2]], before13)
+
+
 def test_pooled_extraction_equals_in_process():
     """generate_conformers_nk maps the per-molecule term extraction over spawned host processes for
     large batches; the terms are the same as in-process."""
