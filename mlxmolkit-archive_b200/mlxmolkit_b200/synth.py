@@ -233,6 +233,25 @@ class SynthMol:
             self._dmat = shortest_path(g, unweighted=True, directed=False)
         return self._dmat
 
+    # Pickled form (molecules travel to the extraction processes): the graph as (i, j, order)
+    # tuples and the conformers as (id, positions); the atom and bond wrappers, neighbour lists
+    # and bond-order map are rebuilt by __init__, the topological distance matrix on first use.
+    _DERIVED = ("_atoms", "nbrs", "border", "_dmat")
+
+    def __getstate__(self) -> dict:
+        st = {k: v for k, v in vars(self).items() if k not in self._DERIVED}
+        st["bonds"] = [(b._i, b._j, b.order) for b in self.bonds]
+        st["_conformers"] = [(c._id, c.pos) for c in self._conformers]
+        return st
+
+    def __setstate__(self, st: dict) -> None:
+        st = dict(st)
+        SynthMol.__init__(self, st.pop("elements"), st.pop("bonds"), st.pop("aromatic"), st.pop("ring_of"),
+                          st.pop("name"))
+        confs = st.pop("_conformers")
+        self.__dict__.update(st)                  # typing results and any attribute set since
+        self._conformers = [SynthConformer(self, cid, pos) for cid, pos in confs]
+
     def copy(self) -> "SynthMol":
         """Fresh copy (graph shared by value, conformers deep-copied)."""
         m = SynthMol(self.elements, [(b._i, b._j, b.order) for b in self.bonds],
