@@ -211,16 +211,17 @@ def _etk_terms(mol_and_bounds):
     return synth_etk_params(mol, bm)
 
 
-def _mmff_terms(mol_and_variant):
-    """MMFF parameters from the molecule's first conformer and the molecule's packed tables, or
-    (None, None) when typing or packing fails."""
+def _mmff_pack(mol_and_variant):
+    """The molecule's packed MMFF tables, typed from its first conformer, or None when typing or
+    packing fails.  Only the tables travel back from a pool process: they hold everything the
+    minimiser reads, the atom count included."""
     from .pack import pack_molecules
     mol, variant = mol_and_variant
     try:
         p = extract_mmff_params(mol, conf_id=mol.GetConformers()[0].GetId(), mmff_variant=variant)
-        return p, pack_molecules([p])
+        return pack_molecules([p])
     except Exception:
-        return None, None
+        return None
 
 
 def _recenter_bounds(b3, pos3: np.ndarray) -> None:
@@ -373,12 +374,12 @@ def generate_conformers_nk(
     # molecules that carry their own conformer are MMFF-typed from it whatever the embedding, so
     # their extraction is queued behind the embedding's host work and runs during its GPU stages
     pre_idx = [i for i in range(N) if not isinstance(smiles_list[i], str)] if run_mmff else []
-    pre_terms = None
+    pre_packs = None
     if dev_idx:
         def queue_mmff():
-            return _pmap_async(_mmff_terms, [(smiles_list[i], mmff_variant) for i in pre_idx]) if pre_idx else None
+            return _pmap_async(_mmff_pack, [(smiles_list[i], mmff_variant) for i in pre_idx]) if pre_idx else None
 
-        confs, ok, en, pre_terms = _embed_on_device(
+        confs, ok, en, pre_packs = _embed_on_device(
             [smiles_list[i] for i in dev_idx], [int(ks[i]) for i in dev_idx], dg_max_iters=dg_max_iters,
             etk_max_iters=etk_max_iters, fourth_dim_weight=fourth_dim_weight, chiral_weight=chiral_weight,
             variant=variant, timings=timings, after_host=queue_mmff)
@@ -395,25 +396,26 @@ def generate_conformers_nk(
     n_batches = 0
     t_mmff = time.perf_counter()
     if run_mmff and N:
-        terms = [None] * N
-        if pre_terms is not None:
-            for i, t in zip(pre_idx, pre_terms()):
-                terms[i] = t
-        rest = [i for i in range(N) if terms[i] is None]
-        for i, t in zip(rest, _pmap(_mmff_terms, [(embedded[i][0], mmff_variant) for i in rest])):
-            terms[i] = t
-        params, packs = [t[0] for t in terms], [t[1] for t in terms]
-        ok = [p is not None and len(xs) > 0 for p, (_, xs) in zip(params, embedded)]
+        packs = [None] * N
+        if pre_packs is not None:
+            for i, k in zip(pre_idx, pre_packs()):
+                packs[i] = k
+        done = set(pre_idx) if pre_packs is not None else set()
+        rest = [i for i in range(N) if i not in done]
+        for i, k in zip(rest, _pmap(_mmff_pack, [(embedded[i][0], mmff_variant) for i in rest])):
+            packs[i] = k
+        ok = [k is not None and len(xs) > 0 for k, (_, xs) in zip(packs, embedded)]
         for i, good in enumerate(ok):
             if not good:
                 results[i].converged = [False] * len(results[i].positions_3d)
         idx = [i for i, g in enumerate(ok) if g]
+        n_at = {i: int(packs[i].n_atoms[0]) for i in idx}
         if idx:
-            max_atoms = max(params[i].n_atoms for i in idx)
+            max_atoms = max(n_at.values())
             iters = mmff_max_iters if mmff_max_iters > 0 else _auto_iters(max_atoms)
             if mmff_use_lbfgs is None:
-                groups = [[i for i in idx if params[i].n_atoms < mm.LBFGS_ATOM_THRESHOLD],
-                          [i for i in idx if params[i].n_atoms >= mm.LBFGS_ATOM_THRESHOLD]]
+                groups = [[i for i in idx if n_at[i] < mm.LBFGS_ATOM_THRESHOLD],
+                          [i for i in idx if n_at[i] >= mm.LBFGS_ATOM_THRESHOLD]]
                 hists = [0, mm.LBFGS_M]
             else:
                 groups, hists = [idx], [mm.LBFGS_M if mmff_use_lbfgs else 0]
@@ -421,13 +423,12 @@ def generate_conformers_nk(
                 if not grp:
                     continue
                 n_batches += 1
-                m = mm.Minimizer([params[i] for i in grp], [len(embedded[i][1]) for i in grp],
-                                 packed=merge_packed([packs[i] for i in grp]))
+                m = mm.Minimizer(None, [len(embedded[i][1]) for i in grp], packed=merge_packed([packs[i] for i in grp]))
                 pos = np.concatenate([np.stack(embedded[i][1]).reshape(-1) for i in grp]).astype(np.float32)
                 r = m.minimize(pos, max_iters=iters, grad_tol=1e-4, history_m=hist)
                 cursor = 0
                 for i in grp:
-                    n = params[i].n_atoms
+                    n = n_at[i]
                     k = len(embedded[i][1])
                     start = int(m.conf_coord[cursor])
                     xyz = r.positions[start: start + 3 * n * k].reshape(k, n, 3).astype(np.float64)

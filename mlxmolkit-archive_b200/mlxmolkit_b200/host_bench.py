@@ -3,7 +3,7 @@ on the CPU alone (no GPU needed).
 
 Each step is what the pipeline does on the host around its GPU stages
 (conformer_pipeline_v2.py): DG terms with the metric-matrix starts (process
-pool), ETK and MMFF term extraction (pool), the 3-D batch with its ETK terms,
+pool), ETK term extraction and MMFF typing + packing (pool), the 3-D batch with its ETK terms,
 the DG and ETK device tables (host threads; also timed on one thread), the
 re-centring of the 1-2 / 1-3 bounds, and the merge of the per-molecule MMFF
 packs.  Seconds are the median of ``--repeats`` after one warm-up pass (which
@@ -38,7 +38,7 @@ def _steps(mols, ks):
 
     dgp, b4, x4 = timed("dg_terms_and_starts", lambda: cp._dg_terms_and_positions(mols, ks, 42, dim=4))
     etk = timed("etk_terms", lambda: cp._pmap(cp._etk_terms, [(m, p.bounds_mat) for m, p in zip(mols, dgp)]))
-    mmff = timed("mmff_terms", lambda: cp._pmap(cp._mmff_terms, [(m, "MMFF94") for m in mols]))
+    mmff = timed("mmff_packs", lambda: cp._pmap(cp._mmff_pack, [(m, "MMFF94") for m in mols]))
     timed("dg_tables", lambda: dg_device_arrays(b4))
     timed("dg_tables_1_thread", lambda: dg_device_arrays(b4, workers=1))
 
@@ -52,7 +52,7 @@ def _steps(mols, ks):
     timed("etk_tables_1_thread", lambda: etk_device_arrays(b3, workers=1))
     x3 = x4.reshape(-1, 4)[:, :3].reshape(-1).copy()
     timed("recentre_bounds", lambda: cp._recenter_bounds(b3, x3))
-    timed("merge_mmff_packs", lambda: merge_packed([k for _, k in mmff if k is not None]))
+    timed("merge_mmff_packs", lambda: merge_packed([k for k in mmff if k is not None]))
     return t
 
 

@@ -152,12 +152,15 @@ class Minimizer:
     """Device-resident minimisation of one packed batch (tables uploaded once)."""
 
     def __init__(self, params_list, conf_counts: Sequence[int], device=None, packed: Optional[PackedBatch] = None):
-        """``packed``: the molecules' tables when already packed (e.g. merged from per-molecule packs)."""
-        self.params_list = list(params_list)
+        """``packed``: the molecules' tables when already packed (e.g. merged from per-molecule
+        packs); ``params_list`` may then be None, the atom counts coming from the tables."""
+        if params_list is None and packed is None:
+            raise ValueError("give the molecules' parameters or their packed tables")
+        self.params_list = list(params_list) if params_list is not None else None
         self.conf_counts = [int(k) for k in conf_counts]
         self.batch = DeviceBatch(packed, device) if packed is not None else \
             DeviceBatch.from_params(self.params_list, device)
-        n_atoms = [int(p.n_atoms) for p in self.params_list]
+        n_atoms = [int(v) for v in packed.n_atoms] if packed is not None else [int(p.n_atoms) for p in self.params_list]
         self.conf_mol, self.conf_coord, self.total = conformer_index(n_atoms, self.conf_counts)
         self.order = lpt_order(n_atoms, self.conf_mol)
         self.confs = DeviceConformers(self.batch, self.conf_mol, self.conf_coord, self.order)

@@ -360,16 +360,16 @@ def test_pooled_extraction_equals_in_process():
             assert np.array_equal(np.asarray(getattr(a, f.name)), np.asarray(getattr(b, f.name))), f.name
     ref = metric_matrix_positions(pack_shared_dg_batch(serial, ks, dim=4), [p.bounds_mat for p in serial], seed=42)
     assert np.array_equal(x4, ref)
+    from mlxmolkit_b200.mmff_params import extract_mmff_params
+    from mlxmolkit_b200.pack import merge_packed, pack_molecules
     items = [(m, "MMFF94s") for m in mols]
-    serial = [cp._mmff_terms(x) for x in items]
-    pooled = cp._pmap(cp._mmff_terms, items)
-    for (pa, ka), (pb, kb) in zip(serial, pooled):
-        for f in fields(pa):
-            assert np.array_equal(np.asarray(getattr(pa, f.name)), np.asarray(getattr(pb, f.name))), f.name
+    serial = [cp._mmff_pack(x) for x in items]
+    pooled = cp._pmap(cp._mmff_pack, items)
+    for ka, kb in zip(serial, pooled):
         for f in fields(ka):
             assert np.array_equal(np.asarray(getattr(ka, f.name)), np.asarray(getattr(kb, f.name))), f.name
-    # the per-molecule packs merge into exactly the tables of packing the list at once
-    from mlxmolkit_b200.pack import merge_packed, pack_molecules
-    whole, merged = pack_molecules([p for p, _ in serial]), merge_packed([k for _, k in pooled])
+    # the per-molecule packs merge into exactly the tables of packing the parameter list at once
+    params = [extract_mmff_params(m, conf_id=m.GetConformers()[0].GetId(), mmff_variant="MMFF94s") for m in mols]
+    whole, merged = pack_molecules(params), merge_packed(pooled)
     for f in fields(whole):
         assert np.array_equal(np.asarray(getattr(whole, f.name)), np.asarray(getattr(merged, f.name))), f.name

@@ -219,7 +219,8 @@ def test_etk_layout_does_not_depend_on_the_thread_split(dg_golden):
         assert set(got) == set(one)
         for f in one:
             if isinstance(one[f], np.ndarray):
-                assert got[f].dtype == one[f].dtype and np.array_equal(got[f].view(np.uint8), one[f].view(np.uint8)), (w, f)
+                assert got[f].dtype == one[f].dtype, (w, f)
+                assert np.array_equal(got[f].view(np.uint8), one[f].view(np.uint8)), (w, f)
             else:
                 assert got[f] == one[f], (w, f)
 
