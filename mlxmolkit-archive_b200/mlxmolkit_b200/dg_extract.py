@@ -253,8 +253,10 @@ def synth_bounds_matrix(mol, conf_id: int = 0) -> np.ndarray:
     for b in mol.GetBonds():
         i, j = b.GetBeginAtomIdx(), b.GetEndAtomIdx()
         path[i, j] = path[j, i] = dist[i, j]
-    for k in range(n):                                   # shortest bond-path lengths (Floyd-Warshall)
-        path = np.minimum(path, path[:, k:k + 1] + path[k:k + 1, :])
+    # shortest bond-path lengths: Floyd-Warshall (the relaxation path[i,k] + path[k,j] in k order;
+    # row and column k do not change in pass k, so in place equals pass by pass, bit for bit)
+    from scipy.sparse.csgraph import floyd_warshall
+    path = np.asarray(floyd_warshall(path, directed=False))
     rad = np.array([_VDW.get(a.GetSymbol(), 1.7) for a in mol.GetAtoms()])
     lb = np.where(topo == 1, dist - 0.01,
          np.where(topo == 2, dist - 0.04,
