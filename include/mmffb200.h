@@ -54,8 +54,11 @@ enum {
     MMFFB_ST_SLOPE = 3,      /* no descent direction (slope >= 0) */
     MMFFB_ST_NONFINITE = 4,  /* energy or gradient not finite */
     MMFFB_ST_LSFAIL = 5,     /* line search found no decrease; position restored */
-    MMFFB_ST_TIMEOUT = 6     /* a bounded wait on a data copy inside the kernel gave up: the
-                                result is not valid; the CTA stopped taking work (never expected) */
+    MMFFB_ST_TIMEOUT = 6     /* no valid result: a bounded wait on a data copy inside the kernel
+                                gave up in this conformer's CTA (positions and energy are those of
+                                the iterate reached), or no CTA reached the conformer afterwards
+                                (energy NaN, 0 iterations, positions as given); the error word is
+                                set (never expected) */
 };
 
 /* arithmetic of the optimizer */
@@ -105,6 +108,14 @@ typedef struct {
                                     energies of the same FP32 coordinates for the line search */
     int32_t hpass_lean;          /* inverse Hessian in global memory: read its column vectors from
                                     shared memory instead of registers (2 CTAs per SM) */
+    uint32_t wait_spins;         /* inverse Hessian in global memory: tests of a row copy's completion
+                                    before its wait gives up (0 = 2^22).  Lowered only to exercise the
+                                    timeout path: 1 gives up whenever the first, non-blocking test
+                                    finds the copy still in flight */
+    int32_t *err_word;           /* optional device int32, zeroed by the call; 1 once the launch is done
+                                    if a bounded wait gave up (the affected conformers then have status
+                                    MMFFB_ST_TIMEOUT).  With or without it, mmffb_minimize's scratch
+                                    keeps the same word at byte 4 */
 } MMFFOptParams;
 
 /* convergence test of mmffb_minimize */
@@ -127,6 +138,19 @@ const char *mmffb_last_error(void);
 int mmffb_energy_grad(const MMFFBatchDev *batch, const MMFFConfDev *confs, int32_t precision,
                       const double *mode, const float *pos, double *energy, float *grad,
                       mmffb_stream_t stream);
+
+/*
+ * FP64 check of returned conformers: each conformer's energy and gradient
+ * re-evaluated in FP64 at pos (typically right after mmffb_minimize, on the
+ * same stream).  e64: float64[n_conf] FP64 energy; err (may be NULL):
+ * energy[c] - e64[c], the returned energy's error against the FP64
+ * evaluation; grad_rms (may be NULL): root mean square of the 3N components of
+ * the FP64 gradient (kcal/mol/A), the stationarity of the returned point.
+ * No counterpart in the reference, whose results carry FP32 energies only
+ * (mlxmolkit/mmff_metal_optimizer.py:34-44, mmff_minimize.py:346).
+ */
+int mmffb_fp64_check(const MMFFBatchDev *batch, const MMFFConfDev *confs, const double *mode, const float *pos,
+                     const double *energy, double *e64, double *err, double *grad_rms, mmffb_stream_t stream);
 
 /* Bytes of device scratch mmffb_minimize needs for these conformers and options. */
 size_t mmffb_minimize_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs,
@@ -178,6 +202,66 @@ int mmffb_fused_sd(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
  */
 int32_t mmffb_pack_chunk(int32_t n_terms, int32_t roles, const int32_t *role_atoms, const int32_t *flip_perm,
                          int32_t n_atoms, int64_t *chunk_out, uint8_t *flipped_out);
+
+/*
+ * Host-side packing of whole batches (no device work; every pointer is host
+ * memory): the device layout above, built from the molecules' extracted term
+ * lists on host threads.  Replaces the reference's per-call host packing
+ * (mlxmolkit/mmff_minimize.py:40-173 _pack_mmff_for_nk,
+ * mlxmolkit/mmff_metal_kernel.py:594-687 pack_multi_mol_for_metal), with one
+ * copy of the tables per molecule instead of one per conformer.
+ *
+ * Input: the MMFFParams fields of n_mols molecules, each field concatenated
+ * over the molecules in molecule order.  term_start[7 * m + t] is the index of
+ * molecule m's first term of type t (bond, angle, stretch-bend, out-of-plane,
+ * torsion, vdW pair, electrostatic pair) in the arrays of that type;
+ * term_start[7 * n_mols + t] is the total.  Atom indices are molecule-local.
+ */
+typedef struct {
+    int32_t n_mols;
+    const int32_t *n_atoms;          /* [n_mols] */
+    const int32_t *diel;             /* [n_mols] ele_diel_model (2: distance-dependent) */
+    const int64_t *term_start;       /* [7 * (n_mols + 1)] */
+    const int32_t *bond_i, *bond_j;
+    const float *bond_kb, *bond_r0;
+    const int32_t *angle_i, *angle_j, *angle_k, *angle_linear;
+    const float *angle_ka, *angle_theta0;
+    const int32_t *sb_i, *sb_j, *sb_k;
+    const float *sb_kba_ijk, *sb_kba_kji, *sb_r0_ij, *sb_r0_kj, *sb_theta0;
+    const int32_t *oop_i, *oop_j, *oop_k, *oop_l;
+    const float *oop_koop;
+    const int32_t *tor_i, *tor_j, *tor_k, *tor_l;
+    const float *tor_v1, *tor_v2, *tor_v3;
+    const int32_t *vdw_i, *vdw_j;
+    const float *vdw_rstar, *vdw_eps;
+    const int32_t *ele_i, *ele_j, *ele_is14;
+    const float *ele_charge;
+    const int64_t *atom_type;        /* [sum n_atoms] MMFF atom type */
+    const double *atom_charge;       /* [sum n_atoms] float64 partial charge */
+} MMFFTermsHost;
+
+typedef struct {
+    int64_t bonded_rows;             /* 16-byte records */
+    int64_t atoms;                   /* atom_cls / atom_q entries */
+    int64_t cls_pairs;               /* (R*, eps) float pairs */
+    int64_t mask_words;
+} MMFFPackSizes;
+
+/*
+ * Pack in two steps.  mmffb_pack_begin builds every molecule's tables on
+ * n_threads host threads (0: all cores), checks them like pack.py does
+ * (vdW parameters a function of the atom types, charge terms float32(q_i q_j),
+ * ...), fills *sizes and returns a handle, or NULL with the reason in
+ * mmffb_last_error().  mmffb_pack_finish writes the batch into the caller's
+ * arrays (mol_desc int32[16 * n_mols], bonded uint32[4 * bonded_rows],
+ * atom_cls int32[atoms], atom_q float64[atoms], cls_tab float32[2 * cls_pairs],
+ * pair_mask uint32[mask_words]) and frees the handle; mmffb_pack_free frees it
+ * unused.
+ */
+void *mmffb_pack_begin(const MMFFTermsHost *terms, int32_t n_threads, MMFFPackSizes *sizes);
+int mmffb_pack_finish(void *handle, int32_t *mol_desc, uint32_t *bonded, int32_t *atom_cls, double *atom_q,
+                      float *cls_tab, uint32_t *pair_mask);
+void mmffb_pack_free(void *handle);
 
 /*
  * The reference's multi-molecule L-BFGS optimizer (mlxmolkit/mmff_metal_optimizer.py:217-535,
@@ -247,9 +331,13 @@ int mmffb_multimol_step(const MMFFBatchDev *batch, const MMFFConfDev *confs, con
  * slot is 3N x 3N elements (N = max_atoms): 4 B each for mixed and fp32,
  * 8 B for fp64.  The call itself allocates nothing.
  *
- * - Set-up: the first call on a device, with that device current, looks up
- *   the array's device address and caches it.  Make that first call before
- *   any stream capture.
+ * - Set-up: every call looks up the array's device address on the current
+ *   device (a lookup, no allocation).  The first call on a device also loads
+ *   this library's module there, so make that first call before any stream
+ *   capture.  Since the lookup is repeated, calls stay valid after a
+ *   cudaDeviceReset.
+ * - Errors inside the launch: the array's error word is not reachable by the
+ *   caller; pass opt->err_word to learn whether a bounded wait gave up.
  * - Limit: if the persistent grid's slots do not all fit in the array, the
  *   grid shrinks to the slots that fit.  Results are unchanged; batches of
  *   large molecules run on fewer CTAs (about 80 for 150 atoms in mixed

@@ -126,6 +126,72 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     return 0;
 }
 
+
+int check_opt(const MMFFOptParams *o) {
+    if (o->max_iters < 0) return fail(MMFFB_EINVAL, "max_iters must be >= 0");
+    if (o->consts[5] < 1) return fail(MMFFB_EINVAL, "MAX_LS must be >= 1");
+    if (o->exit_test != MMFFB_EXIT_TG && o->exit_test != MMFFB_EXIT_ATOM_NORM)
+        return fail(MMFFB_EINVAL, "unknown exit_test %d", o->exit_test);
+    return 0;
+}
+
+Params make_params(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, const Plan &pl,
+                   float *pos, double *energy, int32_t *status, int32_t *iters, int32_t *ls_evals,
+                   unsigned char *scratch) {
+    Params P;
+    memset(&P, 0, sizeof P);
+    P.b = *b;
+    P.c = *c;
+    P.md = to_mode(o->mode);
+    P.K = to_consts(o->consts);
+    P.max_iters = o->max_iters;
+    P.hist_m = o->history_m;
+    P.grad_tol = o->grad_tol;
+    P.exit_test = o->exit_test;
+    P.check_every = o->check_every;
+    P.atom_grad_scale = o->atom_grad_scale;
+    P.max_restarts = o->max_restarts < 0 ? 0 : o->max_restarts;
+    P.polish64 = o->precision == MMFFB_PREC_MIXED && o->polish64 != 0;
+    P.wait_spins = o->wait_spins ? o->wait_spins : kMaxWaitSpins;
+    P.ls_evals = ls_evals;
+    P.nmax = c->max_atoms;
+    P.pos = pos;
+    P.energy = energy;
+    P.status = status;
+    P.iters = iters;
+    P.counter = reinterpret_cast<int *>(scratch);
+    P.err = o->err_word ? reinterpret_cast<int *>(o->err_word) : reinterpret_cast<int *>(scratch) + 1;
+    P.scratch_err = reinterpret_cast<int *>(scratch) + 1;
+    P.gmat = scratch + 256;
+    P.gslot = pl.gslot;
+    return P;
+}
+
+static __global__ void prepare_kernel(const Params P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        *P.counter = 0;
+        *P.err = 0;
+        *P.scratch_err = 0;
+    }
+    for (int i = t; i < P.c.n_conf; i += gridDim.x * blockDim.x) {
+        const int conf = P.c.order ? P.c.order[i] : i;
+        P.status[conf] = MMFFB_ST_TIMEOUT;
+        P.iters[conf] = 0;
+        P.energy[conf] = __longlong_as_double(0x7ff8000000000000LL);   // quiet NaN
+        if (P.ls_evals) P.ls_evals[conf] = 0;
+    }
+}
+
+int prepare_minimize(const Params &P, cudaStream_t st) {
+    int blocks = (P.c.n_conf + 255) / 256;
+    blocks = blocks < 1 ? 1 : (blocks > 148 ? 148 : blocks);
+    prepare_kernel<<<blocks, 256, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "prepare_kernel launch");
+    return 0;
+}
+
 }  // namespace mmffb
 
 using namespace mmffb;
@@ -158,6 +224,23 @@ int mmffb_energy_grad(const MMFFBatchDev *batch, const MMFFConfDev *confs, int32
     return energy_grad_mixed(P, grad, st);
 }
 
+int mmffb_fp64_check(const MMFFBatchDev *batch, const MMFFConfDev *confs, const double *mode, const float *pos,
+                     const double *energy, double *e64, double *err, double *grad_rms, mmffb_stream_t stream) {
+    int r = check_batch(batch, confs);
+    if (r) return r;
+    if (!mode || !pos || !e64) return fail(MMFFB_EINVAL, "null mode, pos or e64");
+    if (err && !energy) return fail(MMFFB_EINVAL, "err needs the returned energies");
+    if (confs->n_conf == 0) return 0;
+    Params P;
+    memset(&P, 0, sizeof P);
+    P.b = *batch;
+    P.c = *confs;
+    P.md = to_mode(mode);
+    P.nmax = confs->max_atoms;
+    P.pos = const_cast<float *>(pos);
+    return check_fp64(P, energy, e64, err, grad_rms, reinterpret_cast<cudaStream_t>(stream));
+}
+
 size_t mmffb_minimize_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs,
                                     const MMFFOptParams *opt) {
     if (check_batch(batch, confs) || !opt) return 0;
@@ -174,10 +257,8 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
     int r = check_batch(batch, confs);
     if (r) return r;
     if (!opt || !pos || !energy || !status || !iters) return fail(MMFFB_EINVAL, "null argument");
-    if (opt->max_iters < 0) return fail(MMFFB_EINVAL, "max_iters must be >= 0");
-    if (opt->consts[5] < 1) return fail(MMFFB_EINVAL, "MAX_LS must be >= 1");
-    if (opt->exit_test != MMFFB_EXIT_TG && opt->exit_test != MMFFB_EXIT_ATOM_NORM)
-        return fail(MMFFB_EINVAL, "unknown exit_test %d", opt->exit_test);
+    r = check_opt(opt);
+    if (r) return r;
     if (confs->n_conf == 0) return 0;
     Plan pl;
     r = plan_minimize(batch, confs, opt, &pl);
@@ -186,32 +267,10 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
     if (!scratch || scratch_bytes < need)
         return fail(MMFFB_ESCRATCH, "scratch of %zu B given, %zu B needed", scratch_bytes, need);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, 256, st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    Params P;
-    memset(&P, 0, sizeof P);
-    P.b = *batch;
-    P.c = *confs;
-    P.md = to_mode(opt->mode);
-    P.K = to_consts(opt->consts);
-    P.max_iters = opt->max_iters;
-    P.hist_m = opt->history_m;
-    P.grad_tol = opt->grad_tol;
-    P.exit_test = opt->exit_test;
-    P.check_every = opt->check_every;
-    P.atom_grad_scale = opt->atom_grad_scale;
-    P.max_restarts = opt->max_restarts < 0 ? 0 : opt->max_restarts;
-    P.polish64 = opt->precision == MMFFB_PREC_MIXED && opt->polish64 != 0;
-    P.ls_evals = ls_evals;
-    P.nmax = confs->max_atoms;
-    P.pos = pos;
-    P.energy = energy;
-    P.status = status;
-    P.iters = iters;
-    P.counter = reinterpret_cast<int *>(scratch);
-    P.err = reinterpret_cast<int *>(scratch) + 1;
-    P.gmat = reinterpret_cast<unsigned char *>(scratch) + 256;
-    P.gslot = pl.gslot;
+    Params P = make_params(batch, confs, opt, pl, pos, energy, status, iters, ls_evals,
+                           reinterpret_cast<unsigned char *>(scratch));
+    r = prepare_minimize(P, st);
+    if (r) return r;
     if (opt->precision == MMFFB_PREC_FP64) return minimize_fp64(P, pl, st);
     if (opt->precision == MMFFB_PREC_FP32) return minimize_fp32(P, pl, st);
     return minimize_mixed(P, pl, st);

@@ -27,4 +27,16 @@ int energy_grad_fp64(const Params &P, float *grad, cudaStream_t st) {
     return launch_eg<double, double, 128>(P, grad, st);
 }
 
+int check_fp64(const Params &P, const double *e_in, double *e64, double *derr, double *grms, cudaStream_t st) {
+    constexpr int NT = 128;
+    Layout L = make_eval_layout(P.nmax, NT / 32, 8, 8, P.b.max_classes);
+    auto k = check64_kernel<NT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    k<<<P.c.n_conf, NT, L.total, st>>>(P, e_in, e64, derr, grms);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "check64_kernel launch");
+    return 0;
+}
+
 }  // namespace mmffb

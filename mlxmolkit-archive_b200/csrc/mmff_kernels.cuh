@@ -82,8 +82,10 @@ struct Params {
     float atom_grad_scale;
     int max_restarts;
     int polish64;      // mixed precision: FP64 line-search energies once the FP32 ones stall
+    uint32_t wait_spins;   // polls before a wait on a ring stage gives up
     int32_t *ls_evals;
-    int *err;          // set when a bounded wait gave up (never expected)
+    int *err;          // set when a bounded wait gave up (never expected): the caller's word or scratch_err
+    int *scratch_err;  // the scratch head's error word (byte 4), set as well
     int nmax;          // largest atom count of the launch (shared-memory layout)
     float *pos;
     double *energy;
@@ -149,6 +151,26 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
     return L;
 }
 
+// Layout of the evaluation-only kernels (energy / gradient, FP64 check): coordinates,
+// per-warp gradient buffers, staged molecule data and the reduction scratch -- none of
+// the optimizer's vectors, so that FP64 evaluations of the largest molecules fit.
+__host__ __device__ inline Layout make_eval_layout(int nmax, int nwarps, size_t rs, size_t as, int max_classes) {
+    Layout L;
+    memset(&L, 0, sizeof L);
+    size_t nv = (size_t)((3 * nmax + 3) & ~3);
+    size_t o = 0;
+    L.pos4 = o; o = al16(o + 4 * (size_t)nmax * rs);
+    L.gbuf = o; o = al16(o + (size_t)nwarps * nv * rs);
+    L.cls = o; o = al16(o + (size_t)nmax * 4);
+    L.q = o; o = al16(o + (size_t)nmax * 8);
+    L.qf = o; o = al16(o + (size_t)nmax * 4);
+    L.mask = o; o = al16(o + 2 * (size_t)nmax * ((nmax + 31) / 32) * 4);
+    L.tab = o; o = al16(o + (size_t)max_classes * max_classes * 8);
+    L.red = o; o = al16(o + 2 * (size_t)nwarps * 8 * as);
+    L.total = o;
+    return L;
+}
+
 __host__ __device__ inline size_t mat_elems(int nmax, int hist_m) {
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
     return hist_m > 0 ? 2 * (size_t)hist_m * nv : (size_t)(3 * nmax) * (size_t)hld(3 * nmax);
@@ -177,6 +199,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {   // non-blocking
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
 // 1-D bulk copy global -> shared (no multicast), completion counted on the mbarrier
 __device__ __forceinline__ void tma_load_row(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -190,8 +221,8 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-constexpr uint32_t kMaxWaitSpins = 1u << 22;   // bounded waits: give up, flag, never hang
-constexpr uint32_t kDrainSpins = 1u << 16;     // bounded wait for copies still in flight after giving up
+constexpr uint32_t kMaxWaitSpins = 1u << 22;   // bounded waits: give up, flag, never hang (default)
+constexpr uint32_t kDrainSpins = 1u << 22;     // bounded wait for copies still in flight after giving up
 
 template <class R> __device__ __forceinline__ R qprod(double a, double b);
 template <> __device__ __forceinline__ float qprod<float>(double a, double b) { return (float)(a * b); }
@@ -578,25 +609,29 @@ struct Opt {
     }
 
     // Warp-uniform bounded wait for ring stage st of this warp.  On giving up it
-    // flags the launch (err word) and this CTA (abort flag) and returns false.
+    // flags the launch (err word) and this CTA (abort flag) and returns false;
+    // the stage's copy may still be in flight (drain() waits for it).
+    // At most P.wait_spins tests: a non-blocking one, then potentially blocking polls.
     __device__ __forceinline__ bool wait_stage(uint64_t *bw, int st) {
-        uint32_t spins = 0;
-        for (;;) {
-            const bool done = mbar_try_wait(&bw[st], (phase >> st) & 1u);
-            if (__all_sync(0xffffffffu, done)) break;
-            if (++spins > kMaxWaitSpins) {
+        const uint32_t par = (phase >> st) & 1u;
+        bool done = mbar_test_wait(&bw[st], par);
+        for (uint32_t spins = 1; !__all_sync(0xffffffffu, done); ++spins) {
+            if (spins >= P.wait_spins) {
                 if ((threadIdx.x & 31) == 0) {
                     atomicExch(P.err, 1);
+                    atomicExch(P.scratch_err, 1);
                     atomicExch(abort_flag, 1);
                 }
                 return false;
             }
+            done = mbar_try_wait(&bw[st], par);
         }
         phase ^= 1u << st;
         return true;
     }
     // After a wait gave up: bounded wait for this warp's copies of rows [from, to) still
-    // in flight, so none lands in shared memory after the CTA has moved on or exited.
+    // in flight -- the row whose wait gave up included -- so none lands in shared
+    // memory after the CTA has moved on or exited.
     __device__ __forceinline__ void drain(uint64_t *bw, int from, int to) {
         for (int t = from; t < to; ++t) {
             const int st = t % kStages;
@@ -689,7 +724,7 @@ struct Opt {
         for (int t = 0; t < nrows; ++t) {
             const int st = t % kStages, i = warp + NW * t;
             if (!wait_stage(bw, st)) {
-                drain(bw, t + 1, nrows < t + kStages ? nrows : t + kStages);
+                drain(bw, t, nrows < t + kStages ? nrows : t + kStages);
                 break;
             }
             const R *src = rw + (size_t)st * ldr;
@@ -773,12 +808,12 @@ struct Opt {
                 const int s0 = t % kStages, s1 = (t + 1) % kStages;
                 const int issued = nrows < t + kStages ? nrows : t + kStages;
                 if (!wait_stage(bw, s0)) {
-                    drain(bw, t + 1, issued);
+                    drain(bw, t, issued);
                     aborted = true;
                     break;
                 }
                 if (two && !wait_stage(bw, s1)) {
-                    drain(bw, t + 2, issued);
+                    drain(bw, t + 1, issued);
                     aborted = true;
                     break;
                 }
@@ -1208,7 +1243,9 @@ __global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_k
         __syncthreads();
         if (item >= P.c.n_conf) break;
         opt.run(order ? order[item] : item);
-        if (*(volatile int *)&s_abort) break;   // a copy never completed: stop taking work
+        // a copy never completed: stop taking work (the conformers left keep the
+        // MMFFB_ST_TIMEOUT that prepare_minimize gave them; healthy CTAs go on)
+        if (*(volatile int *)&s_abort) break;
     }
 }
 
@@ -1221,7 +1258,7 @@ __global__ void __launch_bounds__(NT) energy_grad_kernel(const Params P, float *
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int NW = NT / 32;
     const int conf = blockIdx.x;
-    Layout L = make_layout(P.nmax, NW, 0, false, sizeof(R), sizeof(A), P.b.max_classes);
+    Layout L = make_eval_layout(P.nmax, NW, sizeof(R), sizeof(A), P.b.max_classes);
     R *pos4 = (R *)(smem + L.pos4), *gbuf = (R *)(smem + L.gbuf);
     int *cls = (int *)(smem + L.cls);
     double *qa = (double *)(smem + L.q);
@@ -1252,6 +1289,50 @@ __global__ void __launch_bounds__(NT) energy_grad_kernel(const Params P, float *
     if (threadIdx.x == 0) P.energy[conf] = (double)e[0];
 }
 
+// ---------------------------------------------------------------------------
+// FP64 check of returned conformers: energy and gradient re-evaluated in FP64
+// at the returned coordinates (one CTA per conformer)
+// ---------------------------------------------------------------------------
+
+template <int NT>
+__global__ void __launch_bounds__(NT) check64_kernel(const Params P, const double *e_in, double *e64,
+                                                     double *derr, double *grms) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NW = NT / 32;
+    const int conf = blockIdx.x;
+    Layout L = make_eval_layout(P.nmax, NW, 8, 8, P.b.max_classes);
+    double *pos4 = (double *)(smem + L.pos4), *gbuf = (double *)(smem + L.gbuf);
+    int *cls = (int *)(smem + L.cls);
+    double *qa = (double *)(smem + L.q);
+    float *qf = (float *)(smem + L.qf);
+    uint32_t *mask = (uint32_t *)(smem + L.mask);
+    float2 *tab = (float2 *)(smem + L.tab);
+    double *red = (double *)(smem + L.red);
+    const MolV m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
+    const int n = 3 * m.n, nv = (3 * P.nmax + 3) & ~3;
+    const float *gp = P.pos + P.c.conf_coord[conf];
+    for (int k = threadIdx.x; k < n; k += NT) pos4[4 * (k / 3) + (k % 3)] = (double)gp[k];
+    stage_molecule<NT, false>(P, m, cls, qa, qf, mask, tab);
+    const MolSmem ms{cls, qa, qf, mask, tab};
+    __syncthreads();
+    double s[2], z[1] = {0.0};
+    s[0] = eval_terms<double, double, NW, true, false>(P, m, pos4, gbuf, ms, nv);
+    __syncthreads();
+    s[1] = 0.0;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        double g = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) g += gbuf[(size_t)w * nv + k];
+        s[1] += g * g;
+    }
+    block_reduce<NW, 2, 1, double>(s, z, red);
+    if (threadIdx.x == 0) {
+        e64[conf] = s[0];
+        if (derr) derr[conf] = e_in[conf] - s[0];
+        if (grms) grms[conf] = n > 0 ? sqrt(s[1] / n) : 0.0;
+    }
+}
+
 // launch plan of a minimisation
 struct Plan {
     int nt, nc;
@@ -1275,7 +1356,7 @@ int launch_min(const Params &P, const Plan &pl, cudaStream_t st) {
 
 template <class R, class A, int NT>
 int launch_eg(const Params &P, float *grad, cudaStream_t st) {
-    Layout L = make_layout(P.nmax, NT / 32, 0, false, sizeof(R), sizeof(A), P.b.max_classes);
+    Layout L = make_eval_layout(P.nmax, NT / 32, sizeof(R), sizeof(A), P.b.max_classes);
     auto k = energy_grad_kernel<R, A, NT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
@@ -1322,11 +1403,22 @@ int occupancy_fp32(const Plan &pl, bool lb);
 int energy_grad_mixed(const Params &P, float *grad, cudaStream_t st);
 int energy_grad_fp64(const Params &P, float *grad, cudaStream_t st);
 int energy_grad_fp32(const Params &P, float *grad, cudaStream_t st);
+int check_fp64(const Params &P, const double *e_in, double *e64, double *derr, double *grms, cudaStream_t st);
 
 // argument checks and launch planning shared by the C ABI entry points (mmff_capi.cu)
 int check_batch(const MMFFBatchDev *b, const MMFFConfDev *c);
+int check_opt(const MMFFOptParams *o);
 TermMode to_mode(const double *mode);
 KConst to_consts(const double *k);
 int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, Plan *pl);
+// Params of a minimisation from the options and the caller's buffers (counter and
+// error word in the scratch head, matrix slots from byte 256 of mats).
+Params make_params(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptParams *o, const Plan &pl,
+                   float *pos, double *energy, int32_t *status, int32_t *iters, int32_t *ls_evals,
+                   unsigned char *scratch);
+// Stream-ordered start of a minimisation: zero the work counter and the error word and
+// mark each of the call's conformers MMFFB_ST_TIMEOUT (energy NaN, 0 iterations), so that a
+// conformer no CTA reaches after a bounded wait gave up still has a defined result.
+int prepare_minimize(const Params &P, cudaStream_t st);
 
 }  // namespace mmffb

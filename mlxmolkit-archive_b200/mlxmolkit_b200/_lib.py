@@ -16,7 +16,7 @@ P = ctypes.c_void_p
 
 MMFFB_OK, MMFFB_EINVAL, MMFFB_ECUDA, MMFFB_ESCRATCH, MMFFB_ETOOBIG = 0, -1, -2, -3, -4
 ST_GRAD, ST_MAXIT, ST_TOLX, ST_SLOPE, ST_NONFINITE, ST_LSFAIL, ST_TIMEOUT = 0, 1, 2, 3, 4, 5, 6
-STATUS_NAMES = {0: "grad", 1: "max_iters", 2: "tolx", 3: "slope", 4: "nonfinite", 5: "line_search"}
+STATUS_NAMES = {0: "grad", 1: "max_iters", 2: "tolx", 3: "slope", 4: "nonfinite", 5: "line_search", 6: "timeout"}
 PREC = {"mixed": 0, "fp64": 1, "fp32": 2}
 EXIT_TG, EXIT_ATOM_NORM = 0, 1
 
@@ -39,7 +39,44 @@ class MMFFOptParams(ctypes.Structure):
                 ("consts", ctypes.c_double * 8), ("mode", ctypes.c_double * 4),
                 ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
                 ("atom_grad_scale", ctypes.c_float), ("max_restarts", ctypes.c_int32),
-                ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32)]
+                ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32),
+                ("wait_spins", ctypes.c_uint32), ("err_word", P)]
+
+
+# (MMFFTermsHost field, MMFFParams field, ctypes element type) in the header's order
+TERMS_HOST_FIELDS = [
+    ("bond_i", "bond_idx1", ctypes.c_int32), ("bond_j", "bond_idx2", ctypes.c_int32),
+    ("bond_kb", "bond_kb", ctypes.c_float), ("bond_r0", "bond_r0", ctypes.c_float),
+    ("angle_i", "angle_idx1", ctypes.c_int32), ("angle_j", "angle_idx2", ctypes.c_int32),
+    ("angle_k", "angle_idx3", ctypes.c_int32), ("angle_linear", "angle_is_linear", ctypes.c_int32),
+    ("angle_ka", "angle_ka", ctypes.c_float), ("angle_theta0", "angle_theta0", ctypes.c_float),
+    ("sb_i", "strbend_idx1", ctypes.c_int32), ("sb_j", "strbend_idx2", ctypes.c_int32),
+    ("sb_k", "strbend_idx3", ctypes.c_int32),
+    ("sb_kba_ijk", "strbend_kba_ijk", ctypes.c_float), ("sb_kba_kji", "strbend_kba_kji", ctypes.c_float),
+    ("sb_r0_ij", "strbend_r0_ij", ctypes.c_float), ("sb_r0_kj", "strbend_r0_kj", ctypes.c_float),
+    ("sb_theta0", "strbend_theta0", ctypes.c_float),
+    ("oop_i", "oop_idx1", ctypes.c_int32), ("oop_j", "oop_idx2", ctypes.c_int32),
+    ("oop_k", "oop_idx3", ctypes.c_int32), ("oop_l", "oop_idx4", ctypes.c_int32),
+    ("oop_koop", "oop_koop", ctypes.c_float),
+    ("tor_i", "torsion_idx1", ctypes.c_int32), ("tor_j", "torsion_idx2", ctypes.c_int32),
+    ("tor_k", "torsion_idx3", ctypes.c_int32), ("tor_l", "torsion_idx4", ctypes.c_int32),
+    ("tor_v1", "torsion_V1", ctypes.c_float), ("tor_v2", "torsion_V2", ctypes.c_float),
+    ("tor_v3", "torsion_V3", ctypes.c_float),
+    ("vdw_i", "vdw_idx1", ctypes.c_int32), ("vdw_j", "vdw_idx2", ctypes.c_int32),
+    ("vdw_rstar", "vdw_R_star", ctypes.c_float), ("vdw_eps", "vdw_eps", ctypes.c_float),
+    ("ele_i", "ele_idx1", ctypes.c_int32), ("ele_j", "ele_idx2", ctypes.c_int32),
+    ("ele_is14", "ele_is_1_4", ctypes.c_int32), ("ele_charge", "ele_charge_term", ctypes.c_float),
+]
+
+
+class MMFFTermsHost(ctypes.Structure):
+    _fields_ = [("n_mols", ctypes.c_int32), ("n_atoms", P), ("diel", P), ("term_start", P)] + \
+        [(f, P) for f, _, _ in TERMS_HOST_FIELDS] + [("atom_type", P), ("atom_charge", P)]
+
+
+class MMFFPackSizes(ctypes.Structure):
+    _fields_ = [("bonded_rows", ctypes.c_int64), ("atoms", ctypes.c_int64), ("cls_pairs", ctypes.c_int64),
+                ("mask_words", ctypes.c_int64)]
 
 
 class MMFFMultiMolState(ctypes.Structure):
@@ -80,9 +117,10 @@ class MMFFETKTermsDev(ctypes.Structure):
 
 DG_CONVERGED, DG_MAXIT = 0, 1
 
-EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_minimize_scratch_bytes",
+EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_fp64_check", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_multimol_hist_floats", "mmffb_multimol_step",
+           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_pack_begin", "mmffb_pack_finish", "mmffb_pack_free",
+           "mmffb_multimol_hist_floats", "mmffb_multimol_step",
            "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad",
            "mmffb_etk_scratch_bytes", "mmffb_etk_minimize", "mmffb_etk_energy_grad", "mmffb_stereo_check"]
 
@@ -107,6 +145,8 @@ def load():
     L.mmffb_last_error.restype = ctypes.c_char_p
     L.mmffb_energy_grad.restype = ctypes.c_int
     L.mmffb_energy_grad.argtypes = [BP, CP, ctypes.c_int32, P, P, P, P, P]
+    L.mmffb_fp64_check.restype = ctypes.c_int
+    L.mmffb_fp64_check.argtypes = [BP, CP, P, P, P, P, P, P, P]
     L.mmffb_minimize_scratch_bytes.restype = ctypes.c_size_t
     L.mmffb_minimize_scratch_bytes.argtypes = [BP, CP, OP]
     L.mmffb_minimize.restype = ctypes.c_int
@@ -122,6 +162,12 @@ def load():
     L.mmffb_multimol_step.restype = ctypes.c_int
     L.mmffb_multimol_step.argtypes = [BP, CP, ctypes.POINTER(MMFFMultiMolParams), ctypes.POINTER(MMFFMultiMolState),
                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]
+    L.mmffb_pack_begin.restype = ctypes.c_void_p
+    L.mmffb_pack_begin.argtypes = [ctypes.POINTER(MMFFTermsHost), ctypes.c_int32, ctypes.POINTER(MMFFPackSizes)]
+    L.mmffb_pack_finish.restype = ctypes.c_int
+    L.mmffb_pack_finish.argtypes = [P, P, P, P, P, P, P]
+    L.mmffb_pack_free.restype = None
+    L.mmffb_pack_free.argtypes = [P]
     L.mmffb_pack_chunk.restype = ctypes.c_int32
     L.mmffb_pack_chunk.argtypes = [ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_int32, P, P]
     DBP, DPP = ctypes.POINTER(MMFFDGBatchDev), ctypes.POINTER(MMFFDGParams)

@@ -108,10 +108,15 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                consts=TG_CONSTS, mode=MODE_TG, threads: int = 0, ctas_per_sm: int = 0,
                exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
-               polish64: Optional[bool] = None, hpass_lean: bool = True) -> _lib.MMFFOptParams:
+               polish64: Optional[bool] = None, hpass_lean: bool = True, wait_spins: int = 0,
+               err_word: int = 0) -> _lib.MMFFOptParams:
     """Launch options; ``polish64`` (default: on for mixed precision) switches a conformer's
-    line-search energies to FP64 once the FP32 ones stall."""
+    line-search energies to FP64 once the FP32 ones stall.  ``err_word``: device address of an
+    int32 that the launch sets to 1 when a bounded wait gives up; ``wait_spins`` bounds those
+    waits (0: the library default; lowered only to exercise that path)."""
     o = _lib.MMFFOptParams()
+    o.wait_spins = int(wait_spins)
+    o.err_word = int(err_word) or None
     o.max_restarts = int(max_restarts)
     o.polish64 = int(precision == "mixed" if polish64 is None else bool(polish64))
     o.hpass_lean = int(bool(hpass_lean))
@@ -142,6 +147,11 @@ class MinimizeResult:
     energies: np.ndarray       # float64 (C,)
     status: np.ndarray         # int32 (C,) MMFFB_ST_*
     iters: np.ndarray          # int32 (C,)
+    # FP64 check at the returned coordinates (mmffb_fp64_check): the FP64 energy, the
+    # returned energy's error against it, and the RMS of the FP64 gradient (kcal/mol/A)
+    energies_fp64: Optional[np.ndarray] = None
+    energy_errors: Optional[np.ndarray] = None
+    grad_rms_fp64: Optional[np.ndarray] = None
 
     @property
     def converged(self) -> np.ndarray:
@@ -176,11 +186,14 @@ class Minimizer:
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
-                        hpass_lean: bool = True, stream=None, out=None, evals=None):
+                        hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
+                        wait_spins: int = 0):
         """Minimise in place on the device; returns (energy, status, iters) device tensors.
 
         ``evals`` (optional int32 device tensor, one per conformer) receives the
-        number of energy-only line-search evaluations.
+        number of energy-only line-search evaluations; ``err`` (optional int32
+        device tensor of one element) is set to 1 if a bounded wait inside the
+        kernel gave up (its conformers then have status ``ST_TIMEOUT``).
         """
         torch = _torch()
         L = _lib.load()
@@ -192,7 +205,8 @@ class Minimizer:
         else:
             e, st, it = out
         o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode, threads, ctas_per_sm,
-                       exit_test, check_every, atom_grad_scale, max_restarts, polish64, hpass_lean)
+                       exit_test, check_every, atom_grad_scale, max_restarts, polish64, hpass_lean,
+                       wait_spins, err.data_ptr() if err is not None else 0)
         bd, cd = self.batch.desc(), self.confs.desc()
         nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
         if nbytes == 0 and C > 0:
@@ -206,14 +220,38 @@ class Minimizer:
         return e, st, it
 
     def minimize(self, positions: np.ndarray, **kw) -> MinimizeResult:
+        """Host-synchronous minimisation; raises ``MMFFBError`` if a bounded wait inside the
+        kernel gave up (a result that is not valid, never expected)."""
         torch = _torch()
         pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
         if pos.size != self.total:
             raise ValueError(f"positions hold {pos.size} floats, the conformers need {self.total}")
         pos_dev = torch.from_numpy(pos.copy()).to(self.batch.device)
-        e, st, it = self.minimize_device(pos_dev, **kw)
+        err = torch.zeros(1, dtype=torch.int32, device=self.batch.device)
+        e, st, it = self.minimize_device(pos_dev, err=err, **kw)
+        e64, de, gr = self.fp64_check_device(pos_dev, e, mode=kw.get("mode", MODE_TG))
         torch.cuda.synchronize()
-        return MinimizeResult(pos_dev.cpu().numpy(), e.cpu().numpy(), st.cpu().numpy(), it.cpu().numpy())
+        if int(err.item()):
+            raise _lib.MMFFBError("mmffb_minimize: a bounded wait inside the kernel gave up; "
+                                  f"{int((st == _lib.ST_TIMEOUT).sum().item())} conformers have no valid result")
+        return MinimizeResult(pos_dev.cpu().numpy(), e.cpu().numpy(), st.cpu().numpy(), it.cpu().numpy(),
+                              e64.cpu().numpy(), de.cpu().numpy(), gr.cpu().numpy())
+
+    def fp64_check_device(self, pos_dev, energy_dev, mode=MODE_TG, stream=None):
+        """FP64 energy, error of ``energy_dev`` against it, and FP64 RMS gradient of every
+        conformer at ``pos_dev`` (device tensors, stream-ordered)."""
+        torch = _torch()
+        L = _lib.load()
+        C = self.confs.n_conf
+        e64 = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        de = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        gr = torch.empty(C, dtype=torch.float64, device=self.batch.device)
+        md = (ctypes.c_double * 4)(*[float(v) for v in mode])
+        bd, cd = self.batch.desc(), self.confs.desc()
+        rc = L.mmffb_fp64_check(ctypes.byref(bd), ctypes.byref(cd), md, pos_dev.data_ptr(), energy_dev.data_ptr(),
+                                e64.data_ptr(), de.data_ptr(), gr.data_ptr(), _stream_ptr(torch, stream))
+        _lib.check(rc, "mmffb_fp64_check")
+        return e64, de, gr
 
     def plain_minimize(self, positions: np.ndarray, *, max_iters: int, grad_tol: float = 1e-4,
                        consts=TG_CONSTS, mode=MODE_TG) -> MinimizeResult:
@@ -328,7 +366,8 @@ class BinnedMinimizer(Minimizer):
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
-                        hpass_lean: bool = True, stream=None, out=None, evals=None, time_bins=False):
+                        hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
+                        wait_spins: int = 0, time_bins=False):
         """As ``Minimizer.minimize_device``, one launch per size class.  With
         ``time_bins`` each launch is bracketed by timing events on its own stream;
         ``bin_times_ms()`` reads them after a synchronize."""
@@ -351,7 +390,7 @@ class BinnedMinimizer(Minimizer):
             o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode,
                            threads or cfg.get("threads", 0), ctas_per_sm or cfg.get("ctas_per_sm", 0),
                            exit_test, check_every, atom_grad_scale, max_restarts, polish64,
-                           bool(cfg.get("lean", hpass_lean)))
+                           bool(cfg.get("lean", hpass_lean)), wait_spins, 0)
             cd = b["confs"].desc()
             nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
             if b["scratch"] is None or b["scratch"].numel() < nbytes:
@@ -373,6 +412,13 @@ class BinnedMinimizer(Minimizer):
             ev = torch.cuda.Event()
             ev.record(b["stream"])
             main.wait_event(ev)
+        if err is not None:
+            # each size class's launch keeps its error word at byte 4 of its own scratch
+            # (one shared word would be zeroed by a later class's start)
+            with torch.cuda.stream(main):
+                err.zero_()
+                for b in self.bins:
+                    err.copy_(torch.maximum(err, b["scratch"][4:8].view(torch.int32)))
         return e, st, it
 
     def bin_times_ms(self):

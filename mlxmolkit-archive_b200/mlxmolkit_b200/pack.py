@@ -281,8 +281,70 @@ def _nonbonded(p):
     return tab.reshape(-1, 2), cls.astype(np.int32), q, mask, ncls
 
 
-def pack_molecules(params_list) -> PackedBatch:
-    """Device layout of a list of MMFFParams (one entry per molecule)."""
+_TERM_COUNT_FIELDS = ("bond_idx1", "angle_idx1", "strbend_idx1", "oop_idx1", "torsion_idx1", "vdw_idx1",
+                      "ele_idx1")
+
+
+def pack_molecules(params_list, n_threads: int = 0) -> PackedBatch:
+    """Device layout of a list of MMFFParams (one entry per molecule).
+
+    Built by the native packer of libmmffb200.so (``mmffb_pack_begin`` /
+    ``mmffb_pack_finish``) on ``n_threads`` host threads (0: all cores); the result
+    equals ``pack_molecules_py``'s bit for bit.  Raises ``ValueError`` where that
+    would.
+    """
+    import ctypes
+
+    from . import _lib
+    params_list = list(params_list)
+    M = len(params_list)
+    for p in params_list:
+        if p.atom_type is None or p.partial_charge is None:
+            raise ValueError("non-bonded packing needs per-atom MMFF types and partial charges "
+                             "(MMFFParams.atom_type / partial_charge, filled by extract_mmff_params)")
+    L = _lib.load()
+    keep = []
+
+    def arr(xs, dt):
+        a = np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(1), dtype=dt)
+        if a.size == 0:
+            a = np.zeros(1, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    counts = np.array([[len(getattr(p, f)) for f in _TERM_COUNT_FIELDS] for p in params_list],
+                      dtype=np.int64).reshape(M, 7)
+    starts = np.zeros((M + 1, 7), dtype=np.int64)
+    np.cumsum(counts, axis=0, out=starts[1:])
+    t = _lib.MMFFTermsHost()
+    t.n_mols = M
+    t.n_atoms = arr([np.array([int(p.n_atoms) for p in params_list])], np.int32)
+    t.diel = arr([np.array([int(p.ele_diel_model) for p in params_list])], np.int32)
+    t.term_start = arr([starts.reshape(-1)], np.int64)
+    for cf, pf, ct in _lib.TERMS_HOST_FIELDS:
+        setattr(t, cf, arr([getattr(p, pf) for p in params_list], np.int32 if ct is ctypes.c_int32 else np.float32))
+    t.atom_type = arr([p.atom_type for p in params_list], np.int64)
+    t.atom_charge = arr([p.partial_charge for p in params_list], np.float64)
+    sizes = _lib.MMFFPackSizes()
+    h = L.mmffb_pack_begin(ctypes.byref(t), int(n_threads), ctypes.byref(sizes))
+    if not h:
+        raise ValueError(L.mmffb_last_error().decode(errors="replace"))
+    out = PackedBatch(mol_desc=np.empty((M, MOL_DESC_INTS), np.int32),
+                      bonded=np.empty((sizes.bonded_rows, 4), np.uint32),
+                      atom_cls=np.empty(sizes.atoms, np.int32), atom_q=np.empty(sizes.atoms, np.float64),
+                      cls_tab=np.empty((sizes.cls_pairs, 2), np.float32),
+                      pair_mask=np.empty(sizes.mask_words, np.uint32),
+                      n_atoms=np.asarray([int(p.n_atoms) for p in params_list], dtype=np.int32))
+    rc = L.mmffb_pack_finish(h, out.mol_desc.ctypes.data, out.bonded.ctypes.data, out.atom_cls.ctypes.data,
+                             out.atom_q.ctypes.data, out.cls_tab.ctypes.data, out.pair_mask.ctypes.data)
+    if rc != 0:
+        raise ValueError(L.mmffb_last_error().decode(errors="replace"))
+    return out
+
+
+def pack_molecules_py(params_list) -> PackedBatch:
+    """Device layout of a list of MMFFParams (one entry per molecule): the packing rule in
+    numpy, molecule by molecule (the native packer's specification)."""
     descs, bonded, clss, qs, tabs, masks, natoms = [], [], [], [], [], [], []
     rec_off = atom_off = tab_off = mask_off = 0
     for p in params_list:

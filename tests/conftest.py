@@ -23,6 +23,19 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def golden_large():
+    """Molecules of 130-380 atoms: the dense class above 111 atoms and the L-BFGS sizes."""
+    import numpy as np
+    return np.load(os.path.join(ROOT, "tests", "golden", "ref_mmff_large.npz"))
+
+
+@pytest.fixture(scope="session", params=["drug", "large"])
+def any_golden(request):
+    """Each golden MMFF fixture in turn."""
+    return request.getfixturevalue("golden" if request.param == "drug" else "golden_large")
+
+
+@pytest.fixture(scope="session")
 def dg_golden():
     import numpy as np
     return np.load(os.path.join(ROOT, "tests", "golden", "ref_dg_batches.npz"))

@@ -2,7 +2,7 @@
 
 Run from the repository root with the reference checkout available:
 
-    python tests/golden/make_golden_dg.py /root/reference
+    python tests/golden/make_golden_dg.py <reference-root>
 
 Through the stand-in ``rdkit`` / ``mlx`` modules of ``fake_rdkit.py`` it runs
 the REFERENCE's own mlxmolkit/dg_extract.py (``extract_dg_params``,
@@ -151,4 +151,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden_dg.py <reference-root>")
+    main(sys.argv[1])

@@ -186,3 +186,22 @@ def test_workload_mixture_of_sizes_and_variants():
     _, eo, _, _ = oracle.minimize(params, counts, pos.astype(np.float32).astype(np.float64),
                                   max_iters=3000, consts=oracle.RDKIT_CONSTS)
     assert np.mean(np.abs(r.energies - eo) <= 0.1) >= 0.85, np.abs(r.energies - eo)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_each_returned_energy_carries_its_fp64_check(golden, precision):
+    """mmffb_fp64_check: the FP64 energy and RMS gradient at the returned coordinates equal
+    the FP64 oracle's there, and the returned energy's error against it is recorded."""
+    _, params, counts, pos = _golden_batch(golden)
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos.astype(np.float32), max_iters=500, precision=precision)
+    xs = _split(params, counts, r.positions)
+    pidx = np.repeat(np.arange(len(params)), counts)
+    for c, x in enumerate(xs):
+        eo, go, _ = oracle.energy_grad(params[pidx[c]], x.astype(np.float64))
+        assert abs(r.energies_fp64[c] - eo) <= 1e-11 * max(1.0, abs(eo)), (c, r.energies_fp64[c], eo)
+        rms = np.sqrt(np.mean(go * go))
+        assert abs(r.grad_rms_fp64[c] - rms) <= 1e-9 * max(1e-3, rms), (c, r.grad_rms_fp64[c], rms)
+        assert r.energy_errors[c] == r.energies[c] - r.energies_fp64[c]
+    tol = 1e-5 if precision == "mixed" else 1e-4
+    assert np.all(np.abs(r.energy_errors) <= tol * np.maximum(1.0, np.abs(r.energies_fp64)))

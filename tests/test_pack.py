@@ -170,3 +170,41 @@ def test_native_chunker_equals_the_python_rule():
         a, fa = pack._chunk(ra, fp)
         b, fb = pack.chunk_reference(ra, fp)
         assert np.array_equal(a, b) and np.array_equal(fa, fb)
+
+
+_PACKED_FIELDS = ("mol_desc", "bonded", "atom_cls", "atom_q", "cls_tab", "pair_mask", "n_atoms")
+
+
+@pytest.mark.parametrize("variant", ["MMFF94", "MMFF94s"])
+def test_native_batch_packer_equals_the_python_rule(any_golden, variant):
+    """mmffb_pack_begin/_finish (host threads) produce pack_molecules_py's bytes, on every
+    fixture molecule (16-377 atoms) in one batch and with one thread or many."""
+    g = any_golden
+    params = [extract_mmff_params(golden_mol(g, mi), mmff_variant=variant) for mi in range(int(g["n_mols"]))]
+    _, more, _, _ = small_workload(n_mols=12, k=1, seed=19, lo=4, hi=40)
+    params = params + more
+    ref = pack.pack_molecules_py(params)
+    for nt in (1, 3, 0):
+        got = pack.pack_molecules(params, n_threads=nt)
+        for f in _PACKED_FIELDS:
+            a, b = getattr(ref, f), getattr(got, f)
+            assert a.dtype == b.dtype and a.shape == b.shape, f
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (nt, f)
+
+
+def test_native_batch_packer_edge_cases(golden):
+    empty_ref, empty = pack.pack_molecules_py([]), pack.pack_molecules([])
+    for f in _PACKED_FIELDS:
+        assert np.array_equal(getattr(empty_ref, f), getattr(empty, f)), f
+    p = extract_mmff_params(golden_mol(golden, 2))
+    p.ele_charge_term = p.ele_charge_term.copy()
+    p.ele_charge_term[3] += 1e-3
+    with pytest.raises(ValueError, match="molecule 1: electrostatic charge terms"):
+        pack.pack_molecules([extract_mmff_params(golden_mol(golden, 0)), p])
+    with pytest.raises(ValueError):
+        pack.pack_molecules_py([p])
+    q = extract_mmff_params(golden_mol(golden, 4))
+    q.vdw_idx2 = q.vdw_idx2.copy()
+    q.vdw_idx2[0] = q.vdw_idx1[0]
+    with pytest.raises(ValueError, match="self pair"):
+        pack.pack_molecules([q])

@@ -8,7 +8,8 @@ from oracle import oracle
 
 
 @pytest.mark.parametrize("variant", ["MMFF94", "MMFF94s"])
-def test_extraction_matches_reference_bit_for_bit(golden, variant):
+def test_extraction_matches_reference_bit_for_bit(any_golden, variant):
+    golden = any_golden
     for mi in range(int(golden["n_mols"])):
         mol = golden_mol(golden, mi)
         mine = extract_mmff_params(mol, mmff_variant=variant)
@@ -21,7 +22,8 @@ def test_extraction_matches_reference_bit_for_bit(golden, variant):
         assert mine.ele_diel_model == int(golden[f"m{mi}_{variant}_ele_diel_model"])
 
 
-def test_variants_differ_only_where_mmff94s_changes_terms(golden):
+def test_variants_differ_only_where_mmff94s_changes_terms(any_golden):
+    golden = any_golden
     changed = 0
     for mi in range(int(golden["n_mols"])):
         for f in TERM_FIELDS:
@@ -33,8 +35,9 @@ def test_variants_differ_only_where_mmff94s_changes_terms(golden):
 
 
 @pytest.mark.parametrize("variant", ["MMFF94", "MMFF94s"])
-def test_oracle_energy_matches_reference_numpy(golden, variant):
+def test_oracle_energy_matches_reference_numpy(any_golden, variant):
     """FP64 oracle in the mega/numpy constant mode == mmff_energy_vectorized (fixture)."""
+    golden = any_golden
     for mi in range(int(golden["n_mols"])):
         p = golden_params(golden, mi, variant)
         pos = golden[f"m{mi}_pos"]
@@ -47,8 +50,9 @@ def test_oracle_energy_matches_reference_numpy(golden, variant):
             assert np.abs(g.astype(np.float32) - ref_g[c]).max() <= 1e-6 * scale, (mi, c)
 
 
-def test_oracle_gradient_is_the_derivative_of_its_energy(golden):
+def test_oracle_gradient_is_the_derivative_of_its_energy(any_golden):
     """Central differences of the FP64 oracle energy, TG-header constants, every term type."""
+    golden = any_golden
     rng = np.random.default_rng(0)
     for mi in range(int(golden["n_mols"])):
         p = golden_params(golden, mi)

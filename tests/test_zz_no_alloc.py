@@ -1,8 +1,12 @@
 """mmffb_minimize_noalloc (fixed device scratch, no allocation) against mmffb_minimize.
 
-The file name sorts last so it also runs after every other GPU test in one
-process: the fixed array is then reused, and the entry point must zero the work
-counter and the error word itself.
+The fixed array keeps whatever the previous call left in it, so each parity
+check first leaves it dirty itself -- a call on another batch ends with a
+non-zero work counter, and a call whose bounded waits give up sets the error
+word -- and the entry point must start both at zero again.  The file name also
+sorts last, so in a full run it comes after every other GPU test.  (The
+MMFFB_ESCRATCH branch, one inverse-Hessian slot larger than the array, cannot
+be reached: the largest dense slot, 170 atoms in FP64, is 2 MiB of the 64.)
 """
 import ctypes
 
@@ -31,6 +35,7 @@ def _large_batch(n_conf=160, seed=11):
 
 
 def _noalloc(m, pos_dev, opt):
+    """One mmffb_minimize_noalloc call; returns (energy, status, iters, ls_evals)."""
     import torch
     L = _lib.load()
     C = m.confs.n_conf
@@ -52,7 +57,27 @@ def _scratch_bytes(m, opt):
     return L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(opt))
 
 
-@pytest.mark.parametrize("case,precision", [("large", "mixed"), ("large", "fp64"), ("small", "mixed")])
+def _dirty_the_array():
+    """Leave the fixed array as an earlier caller might: a finished call on another batch
+    (work counter at its conformer count plus its grid) and a call whose bounded waits gave
+    up (error word set)."""
+    import torch
+    _, params, counts, pos = small_workload(n_mols=3, k=5, seed=41)
+    m = mm.Minimizer(params, counts)
+    x = torch.from_numpy(pos.astype(np.float32)).cuda()
+    _noalloc(m, x, mm.opt_params(max_iters=20, grad_tol=1e-4))
+    params, counts, pos = _large_batch(n_conf=8, seed=13)
+    m = mm.Minimizer(params, counts)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    x = torch.from_numpy(pos.astype(np.float32)).cuda()
+    _, st, _, _ = _noalloc(m, x, mm.opt_params(max_iters=20, grad_tol=1e-4, wait_spins=1,
+                                               err_word=err.data_ptr()))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1 and bool((st == _lib.ST_TIMEOUT).all())
+
+
+@pytest.mark.parametrize("case,precision", [("large", "mixed"), ("large", "fp64"), ("large", "fp32"),
+                                            ("small", "mixed"), ("small", "fp32")])
 def test_noalloc_matches_mmffb_minimize_over_two_calls_in_a_row(case, precision):
     import torch
     if case == "large":
@@ -61,20 +86,23 @@ def test_noalloc_matches_mmffb_minimize_over_two_calls_in_a_row(case, precision)
         _, params, counts, pos = small_workload(n_mols=6, k=4, seed=21)
     m = mm.Minimizer(params, counts)
     kw = dict(max_iters=300, grad_tol=1e-4, precision=precision)
-    opt = mm.opt_params(**kw)
     if case == "large":
         # the planned grid's slots exceed the fixed array, so the grid shrinks
-        assert _scratch_bytes(m, opt) > NOALLOC_BYTES
+        assert _scratch_bytes(m, mm.opt_params(**kw)) > NOALLOC_BYTES
     start = torch.from_numpy(pos.astype(np.float32)).cuda()
 
     x_ref = start.clone()
     ev_ref = torch.empty(m.confs.n_conf, dtype=torch.int32, device="cuda")
     e_ref, st_ref, it_ref = m.minimize_device(x_ref, evals=ev_ref, **kw)
 
+    _dirty_the_array()
+    err = torch.full((1,), 5, dtype=torch.int32, device="cuda")
+    opt = mm.opt_params(**kw, err_word=err.data_ptr())
     x1, x2 = start.clone(), start.clone()
     r1 = _noalloc(m, x1, opt)
     r2 = _noalloc(m, x2, opt)          # queued right behind the first on the same stream
     torch.cuda.synchronize()
+    assert int(err.item()) == 0
     ref = [t.cpu().numpy() for t in (x_ref, e_ref, st_ref, it_ref, ev_ref)]
     for x, r in ((x1, r1), (x2, r2)):
         got = [t.cpu().numpy() for t in (x, *r)]
