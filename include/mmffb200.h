@@ -109,9 +109,15 @@ typedef struct {
     int32_t hpass_lean;          /* inverse Hessian in global memory: read its column vectors from
                                     shared memory instead of registers (2 CTAs per SM) */
     uint32_t wait_spins;         /* inverse Hessian in global memory: tests of a row copy's completion
-                                    before its wait gives up (0 = 2^22).  Lowered only to exercise the
-                                    timeout path: 1 gives up whenever the first, non-blocking test
-                                    finds the copy still in flight */
+                                    before its wait gives up (0 = 2^22) */
+    int32_t give_up_waits;       /* test switch, 0 in normal use: 1 = every wait for a row copy gives up
+                                    before testing, as if the copy never completed, which exercises the
+                                    timeout path (the kernel drains the copies in flight, its conformers
+                                    end MMFFB_ST_TIMEOUT and the error word is set) */
+    int32_t two_pending;         /* inverse Hessian in global memory, register-lean mixed instance: 0 = keep
+                                    two rank-2 updates pending and store H every other iteration when the
+                                    extra shared memory leaves as many CTAs per SM (same results, half the
+                                    write-back); -1 = store after every update */
     int32_t *err_word;           /* optional device int32, zeroed by the call; 1 once the launch is done
                                     if a bounded wait gave up (the affected conformers then have status
                                     MMFFB_ST_TIMEOUT).  With or without it, mmffb_minimize's scratch
@@ -311,6 +317,46 @@ size_t mmffb_multimol_hist_floats(const MMFFConfDev *confs, int32_t history_m);
 int mmffb_multimol_step(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFMultiMolParams *params,
                         const MMFFMultiMolState *state, int32_t phase, int32_t n_iters, int32_t it_end,
                         int32_t max_iters, mmffb_stream_t stream);
+
+/*
+ * Serving worker: one persistent launch of the minimiser that takes conformer
+ * slots from a work queue while it runs, so that conformers published while
+ * others are being optimised start as soon as a CTA frees up.  No counterpart
+ * in the reference, whose multi-molecule loop runs each batch in lockstep
+ * (mlxmolkit/mmff_metal_optimizer.py:255-260).
+ *
+ * The queue's slots are the conformers of confs (n_conf = capacity, order
+ * NULL): slot s is conformer s of the arrays there and of pos / energy /
+ * status / iters.  The host publishes slots in index order by writing, after
+ * the slots' tables, descriptors and coordinates are in device memory, the
+ * number of published slots to *tail with a copy ordered on the stream that
+ * carried that data (never on the worker's stream).  The launch claims slots
+ * from *head, writes each slot's results, then sets done[s] = 1 in host
+ * memory.  It ends when *close is set and every published slot is claimed,
+ * or after idle_polls polls of an empty queue (sleep_ns apart): every wait is
+ * bounded.  Device memory that a running worker has read must not be written
+ * again until it ends (the caches of a launch are not refreshed).
+ */
+typedef struct {
+    int32_t *head;           /* device int32: next slot to claim; zero before the queue's first launch */
+    const int32_t *tail;     /* device int32: slots published */
+    const int32_t *close;    /* device int32: nonzero once no more slots will be published */
+    int32_t *done;           /* int32[capacity] of host memory mapped for the device (cudaHostAlloc
+                                with cudaHostAllocMapped; its device address) */
+    uint32_t idle_polls;     /* empty polls before the launch ends */
+    uint32_t sleep_ns;       /* pause between empty polls */
+} MMFFQueueDev;
+
+/* Host memory the device can write (for MMFFQueueDev.done): zeroed; *device is its device address. */
+int mmffb_host_alloc_mapped(size_t bytes, void **host, void **device);
+int mmffb_host_free(void *host);
+
+/* Bytes of device scratch mmffb_minimize_queue needs (max_ctas: 0 = as many CTAs as fit). */
+size_t mmffb_queue_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                                 int32_t max_ctas);
+int mmffb_minimize_queue(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                         const MMFFQueueDev *queue, float *pos, double *energy, int32_t *status, int32_t *iters,
+                         int32_t max_ctas, void *scratch, size_t scratch_bytes, mmffb_stream_t stream);
 
 /* Size of the fixed per-device scratch array behind mmffb_minimize_noalloc. */
 #define MMFFB_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)

@@ -112,12 +112,31 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     pl->nt = nt;
     pl->nc = nc;
     pl->msm = msm;
+    pl->two_pend = false;
     pl->smem = L.total;
     pl->rsz = rs;
     pl->gslot = mat_elems(nmax, o->history_m);
-    int fit = o->precision == MMFFB_PREC_FP64 ? occupancy_fp64(*pl, lb)
-            : o->precision == MMFFB_PREC_FP32 ? occupancy_fp32(*pl, lb) : occupancy_mixed(*pl, lb);
+    auto occupancy = [&]() {
+        return o->precision == MMFFB_PREC_FP64 ? occupancy_fp64(*pl, lb)
+             : o->precision == MMFFB_PREC_FP32 ? occupancy_fp32(*pl, lb) : occupancy_mixed(*pl, lb);
+    };
+    int fit = occupancy();
     if (fit < 0) return fit;
+    if (mixed && !lb && !msm && nc == 0 && o->two_pending >= 0) {
+        // the register-lean streamed instance: keep two updates pending and store H every
+        // other iteration, when the three extra vectors still leave as many CTAs per SM
+        Layout L2 = make_layout(nmax, nt / 32, 0, false, rs, as, mc, true);
+        pl->smem = L2.total;
+        pl->two_pend = true;
+        const int fit2 = L2.total <= (size_t)optin ? occupancy() : 0;
+        if (fit2 < 0) return fit2;
+        if (fit2 >= fit && fit2 > 0) {
+            fit = fit2;
+        } else {
+            pl->smem = L.total;
+            pl->two_pend = false;
+        }
+    }
     if (fit < 1) return fail(MMFFB_ETOOBIG, "no CTA of this instance fits on an SM (%zu B shared)", pl->smem);
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
     int grid = sms * fit;
@@ -152,7 +171,8 @@ Params make_params(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPar
     P.atom_grad_scale = o->atom_grad_scale;
     P.max_restarts = o->max_restarts < 0 ? 0 : o->max_restarts;
     P.polish64 = o->precision == MMFFB_PREC_MIXED && o->polish64 != 0;
-    P.wait_spins = o->wait_spins ? o->wait_spins : kMaxWaitSpins;
+    P.wait_spins = o->give_up_waits ? 0u : o->wait_spins ? o->wait_spins : kMaxWaitSpins;
+    P.two_pending = pl.two_pend ? 1 : 0;
     P.ls_evals = ls_evals;
     P.nmax = c->max_atoms;
     P.pos = pos;
@@ -165,6 +185,11 @@ Params make_params(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPar
     P.gmat = scratch + 256;
     P.gslot = pl.gslot;
     return P;
+}
+
+static __global__ void zero_err_kernel(const Params P) {
+    *P.err = 0;
+    *P.scratch_err = 0;
 }
 
 static __global__ void prepare_kernel(const Params P) {
@@ -271,6 +296,70 @@ int mmffb_minimize(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MM
                            reinterpret_cast<unsigned char *>(scratch));
     r = prepare_minimize(P, st);
     if (r) return r;
+    if (opt->precision == MMFFB_PREC_FP64) return minimize_fp64(P, pl, st);
+    if (opt->precision == MMFFB_PREC_FP32) return minimize_fp32(P, pl, st);
+    return minimize_mixed(P, pl, st);
+}
+
+int mmffb_host_alloc_mapped(size_t bytes, void **host, void **device) {
+    if (!host || !device || bytes == 0) return fail(MMFFB_EINVAL, "null pointer or zero size");
+    cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocMapped);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc(mapped)");
+    std::memset(*host, 0, bytes);
+    e = cudaHostGetDevicePointer(device, *host, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(*host);
+        *host = nullptr;
+        return cuda_fail(e, "cudaHostGetDevicePointer");
+    }
+    return 0;
+}
+
+int mmffb_host_free(void *host) {
+    cudaError_t e = cudaFreeHost(host);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "cudaFreeHost");
+}
+
+size_t mmffb_queue_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                                 int32_t max_ctas) {
+    if (check_batch(batch, confs) || !opt) return 0;
+    Plan pl;
+    if (plan_minimize(batch, confs, opt, &pl)) return 0;
+    if (max_ctas > 0 && pl.grid > max_ctas) pl.grid = max_ctas;
+    return 256 + (pl.msm ? 0 : (size_t)pl.grid * pl.gslot * pl.rsz);
+}
+
+int mmffb_minimize_queue(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
+                         const MMFFQueueDev *queue, float *pos, double *energy, int32_t *status, int32_t *iters,
+                         int32_t max_ctas, void *scratch, size_t scratch_bytes, mmffb_stream_t stream) {
+    int r = check_batch(batch, confs);
+    if (r) return r;
+    if (!opt || !queue || !pos || !energy || !status || !iters) return fail(MMFFB_EINVAL, "null argument");
+    if (!queue->head || !queue->tail || !queue->close || !queue->done)
+        return fail(MMFFB_EINVAL, "null queue pointer");
+    if (confs->order) return fail(MMFFB_EINVAL, "queue slots are taken in index order (order must be NULL)");
+    r = check_opt(opt);
+    if (r) return r;
+    if (confs->n_conf == 0) return 0;
+    Plan pl;
+    r = plan_minimize(batch, confs, opt, &pl);
+    if (r) return r;
+    if (max_ctas > 0 && pl.grid > max_ctas) pl.grid = max_ctas;
+    const size_t need = 256 + (pl.msm ? 0 : (size_t)pl.grid * pl.gslot * pl.rsz);
+    if (!scratch || scratch_bytes < need)
+        return fail(MMFFB_ESCRATCH, "scratch of %zu B given, %zu B needed", scratch_bytes, need);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    Params P = make_params(batch, confs, opt, pl, pos, energy, status, iters, nullptr,
+                           reinterpret_cast<unsigned char *>(scratch));
+    P.q_head = queue->head;
+    P.q_tail = queue->tail;
+    P.q_close = queue->close;
+    P.q_done = queue->done;
+    P.q_idle_polls = queue->idle_polls;
+    P.q_sleep_ns = queue->sleep_ns;
+    zero_err_kernel<<<1, 1, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "zero_err_kernel launch");
     if (opt->precision == MMFFB_PREC_FP64) return minimize_fp64(P, pl, st);
     if (opt->precision == MMFFB_PREC_FP32) return minimize_fp32(P, pl, st);
     return minimize_mixed(P, pl, st);

@@ -82,7 +82,8 @@ struct Params {
     float atom_grad_scale;
     int max_restarts;
     int polish64;      // mixed precision: FP64 line-search energies once the FP32 ones stall
-    uint32_t wait_spins;   // polls before a wait on a ring stage gives up
+    uint32_t wait_spins;   // tests of a ring stage's completion before its wait gives up (0: none)
+    int two_pending;   // streamed FP32 H: store it every other iteration, two updates pending
     int32_t *ls_evals;
     int *err;          // set when a bounded wait gave up (never expected): the caller's word or scratch_err
     int *scratch_err;  // the scratch head's error word (byte 4), set as well
@@ -94,7 +95,37 @@ struct Params {
     void *gmat;        // per-CTA global matrix slots (when not in shared memory)
     size_t gslot;      // elements per slot
     int *counter;      // work counter
+    // work queue of a serving worker (q_tail != nullptr): conformer slots are published by the
+    // host while the launch runs (tail), claimed here (head) and flagged done in host memory
+    int *q_head;
+    const int *q_tail;
+    const int *q_close;
+    int *q_done;
+    uint32_t q_idle_polls;
+    uint32_t q_sleep_ns;
 };
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The next published conformer slot of a serving worker, or -1 once the queue is closed
+// and drained, or after q_idle_polls empty polls (q_sleep_ns apart): bounded, never hangs.
+__device__ __forceinline__ int claim_slot(const Params &P) {
+    for (uint32_t polls = 0;; ++polls) {
+        const int t = ld_acquire_gpu(P.q_tail);
+        const int h = *(volatile int *)P.q_head;
+        if (h < t) {
+            if (atomicCAS(P.q_head, h, h + 1) == h) return h;
+            continue;
+        }
+        if (ld_acquire_gpu(P.q_close)) return -1;
+        if (polls >= P.q_idle_polls) return -1;
+        __nanosleep(P.q_sleep_ns);
+    }
+}
 
 __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
@@ -102,15 +133,15 @@ __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(
 constexpr int kStages = 4;         // rows of H in flight per warp (TMA ring)
 
 struct Layout {
-    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, qf, mask, tab, red, rho, alpha,
-        ring, mbar, mat, total;
+    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, pxi2, pc2, pr2, gbuf, cls, q, qf, mask, tab, red,
+        rho, alpha, ring, mbar, mat, total;
 };
 
 // row stride of a dense inverse Hessian in global memory: 16-byte multiple for TMA rows
 __host__ __device__ __forceinline__ int hld(int n) { return (n + 3) & ~3; }
 
 __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, bool mat_in_smem,
-                                              size_t rs, size_t as, int max_classes = 32) {
+                                              size_t rs, size_t as, int max_classes = 32, bool two_pend = false) {
     Layout L;
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
     size_t o = 0;
@@ -126,6 +157,9 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
     L.pxi = o; o = al16(o + nv * rs);
     L.pc = o; o = al16(o + nv * rs);
     L.pr = o; o = al16(o + nv * rs);
+    L.pxi2 = o; o = al16(o + (two_pend ? nv * rs : 0));   // the second pending update
+    L.pc2 = o; o = al16(o + (two_pend ? nv * rs : 0));
+    L.pr2 = o; o = al16(o + (two_pend ? nv * rs : 0));
     L.gbuf = o; o = al16(o + (size_t)nwarps * nv * rs);
     L.cls = o; o = al16(o + (size_t)nmax * 4);
     L.q = o; o = al16(o + (size_t)nmax * 8);
@@ -510,8 +544,10 @@ __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>
 struct Opt {
     static constexpr int NW = NT / 32;
+    // the register-lean streamed FP32 instance may keep two updates pending (P.two_pending)
+    static constexpr bool kTwoPend = !MSM && NC == 0 && sizeof(R) == 4 && !LB;
     const Params &P;
-    R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *gbuf, *mat;
+    R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *pxi2, *pc2, *pr2, *gbuf, *mat;
     double *pos4d;     // FP64 copy of pos4 (float R only)
     R *ring;           // TMA row ring (streamed H pass)
     uint64_t *mbar;    // one mbarrier per ring stage and warp
@@ -531,7 +567,8 @@ struct Opt {
     int N, n, nv;
 
     __device__ Opt(const Params &p, unsigned char *sm, int *abort_ = nullptr) : P(p), abort_flag(abort_), rsel(0) {
-        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes);
+        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes,
+                               p.two_pending != 0);
         pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
         pos4d = (double *)(sm + L.pos4d);
         use64 = false;
@@ -541,6 +578,7 @@ struct Opt {
         ldh = 0;
         xo = (R *)(sm + L.xo); dg = (R *)(sm + L.dg); hp = (R *)(sm + L.hp); hq = (R *)(sm + L.hq);
         pxi = (R *)(sm + L.pxi); pc = (R *)(sm + L.pc); pr = (R *)(sm + L.pr); gbuf = (R *)(sm + L.gbuf);
+        pxi2 = (R *)(sm + L.pxi2); pc2 = (R *)(sm + L.pc2); pr2 = (R *)(sm + L.pr2);
         cls = (int *)(sm + L.cls); qa = (double *)(sm + L.q); red = (A *)(sm + L.red);
         qf = (float *)(sm + L.qf); mask = (uint32_t *)(sm + L.mask); tab = (float2 *)(sm + L.tab);
         ms.cls = cls; ms.qa = qa; ms.qf = qf; ms.mask = mask; ms.tab = tab;
@@ -611,10 +649,11 @@ struct Opt {
     // Warp-uniform bounded wait for ring stage st of this warp.  On giving up it
     // flags the launch (err word) and this CTA (abort flag) and returns false;
     // the stage's copy may still be in flight (drain() waits for it).
-    // At most P.wait_spins tests: a non-blocking one, then potentially blocking polls.
+    // At most P.wait_spins tests: a non-blocking one, then potentially blocking polls
+    // (none when P.wait_spins is 0: the wait gives up at once).
     __device__ __forceinline__ bool wait_stage(uint64_t *bw, int st) {
         const uint32_t par = (phase >> st) & 1u;
-        bool done = mbar_test_wait(&bw[st], par);
+        bool done = P.wait_spins > 0 && mbar_test_wait(&bw[st], par);
         for (uint32_t spins = 1; !__all_sync(0xffffffffu, done); ++spins) {
             if (spins >= P.wait_spins) {
                 if ((threadIdx.x & 31) == 0) {
@@ -777,7 +816,13 @@ struct Opt {
     // rows of H and the vectors are padded to a multiple of 4 with zeros) and two
     // rows per step, so each vector load from shared memory serves two rows and a
     // warp keeps two row copies of its TMA ring in use at once.
-    __device__ __forceinline__ void hpass_stream_v4(bool pending) {
+    //
+    // npend rank-2 updates are pending (0, 1 or 2; the older in pxi/pc/pr, the newer
+    // in pxi2/pc2/pr2) and applied to each element in that order, so the values equal
+    // those of storing after every update; the rows are stored only when `store`.
+    // With two pending updates stored every other iteration, H is written back half
+    // as often for the same results.
+    __device__ __forceinline__ void hpass_stream_v4(int npend, bool store) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int ldr = hld(3 * P.nmax);
         float *rw = (float *)ring + (size_t)warp * kStages * ldr;
@@ -786,6 +831,7 @@ struct Opt {
         const uint32_t bytes = (uint32_t)(ldh * sizeof(float));
         const int n4 = ldh >> 2;
         const float4 *X4 = (const float4 *)pxi, *C4 = (const float4 *)pc;
+        const float4 *Y4 = (const float4 *)pxi2, *D24 = (const float4 *)pc2;
         const float4 *G4 = (const float4 *)g, *D4 = (const float4 *)dg;
         float *H = (float *)mat;
         if (lane == 0) {
@@ -820,34 +866,52 @@ struct Opt {
                 const int i0 = warp + NW * t, i1 = i0 + NW;
                 const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
                 float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
-                const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
-                const float r1 = (pending && two) ? (float)pr[i1] : 0.f, x1 = (pending && two) ? (float)pxi[i1] : 0.f;
-                float a0 = 0.f, q0 = 0.f, a1 = 0.f, q1 = 0.f;
+                const bool p1 = npend >= 1, p2 = npend >= 2;
+                const float r0 = p1 ? (float)pr[i0] : 0.f, x0 = p1 ? (float)pxi[i0] : 0.f;
+                const float r1 = (p1 && two) ? (float)pr[i1] : 0.f, x1 = (p1 && two) ? (float)pxi[i1] : 0.f;
+                const float q0 = p2 ? (float)pr2[i0] : 0.f, y0 = p2 ? (float)pxi2[i0] : 0.f;
+                const float q1 = (p2 && two) ? (float)pr2[i1] : 0.f, y1 = (p2 && two) ? (float)pxi2[i1] : 0.f;
+                float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
                 for (int c = lane; c < n4; c += 32) {
                     float4 h0 = A0[c];
                     float4 h1 = two ? A1[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (pending) {
+                    if (p1) {
                         const float4 px = X4[c], pv = C4[c];
                         h0.x = fmaf(x0, pv.x, fmaf(px.x, r0, h0.x));
                         h0.y = fmaf(x0, pv.y, fmaf(px.y, r0, h0.y));
                         h0.z = fmaf(x0, pv.z, fmaf(px.z, r0, h0.z));
                         h0.w = fmaf(x0, pv.w, fmaf(px.w, r0, h0.w));
-                        W0[c] = h0;
                         if (two) {
                             h1.x = fmaf(x1, pv.x, fmaf(px.x, r1, h1.x));
                             h1.y = fmaf(x1, pv.y, fmaf(px.y, r1, h1.y));
                             h1.z = fmaf(x1, pv.z, fmaf(px.z, r1, h1.z));
                             h1.w = fmaf(x1, pv.w, fmaf(px.w, r1, h1.w));
-                            W1[c] = h1;
                         }
+                    }
+                    if (p2) {
+                        const float4 py = Y4[c], pw = D24[c];
+                        h0.x = fmaf(y0, pw.x, fmaf(py.x, q0, h0.x));
+                        h0.y = fmaf(y0, pw.y, fmaf(py.y, q0, h0.y));
+                        h0.z = fmaf(y0, pw.z, fmaf(py.z, q0, h0.z));
+                        h0.w = fmaf(y0, pw.w, fmaf(py.w, q0, h0.w));
+                        if (two) {
+                            h1.x = fmaf(y1, pw.x, fmaf(py.x, q1, h1.x));
+                            h1.y = fmaf(y1, pw.y, fmaf(py.y, q1, h1.y));
+                            h1.z = fmaf(y1, pw.z, fmaf(py.z, q1, h1.z));
+                            h1.w = fmaf(y1, pw.w, fmaf(py.w, q1, h1.w));
+                        }
+                    }
+                    if (store) {
+                        W0[c] = h0;
+                        if (two) W1[c] = h1;
                     }
                     const float4 gg = G4[c], dd = D4[c];
                     a0 = fmaf(h0.w, gg.w, fmaf(h0.z, gg.z, fmaf(h0.y, gg.y, fmaf(h0.x, gg.x, a0))));
-                    q0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, q0))));
+                    b0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, b0))));
                     a1 = fmaf(h1.w, gg.w, fmaf(h1.z, gg.z, fmaf(h1.y, gg.y, fmaf(h1.x, gg.x, a1))));
-                    q1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, q1))));
+                    b1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, b1))));
                 }
-                v[4 * u] = a0; v[4 * u + 1] = q0; v[4 * u + 2] = a1; v[4 * u + 3] = q1;
+                v[4 * u] = a0; v[4 * u + 1] = b0; v[4 * u + 2] = a1; v[4 * u + 3] = b1;
                 __syncwarp();   // every lane's reads of both stages before they are refilled
                 if (lane == 0) {
                     fence_proxy_async_smem();
@@ -864,7 +928,7 @@ struct Opt {
                 }
             }
             if (aborted) break;
-            // lanes l and l^1 now hold the sum of value l >> 1: pair u = value / 4, then a0 q0 a1 q1
+            // lanes l and l^1 now hold the sum of value l >> 1: pair u = value / 4, then a0 b0 a1 b1
             const float sum = reduce16(v);
             const int val = lane >> 1, tr = t0 + 2 * (val >> 2) + ((val >> 1) & 1);
             if (!(lane & 1) && tr < nrows) {
@@ -946,7 +1010,10 @@ struct Opt {
         stage_molecule<NT, sizeof(R) == 4>(P, m, cls, qa, qf, mask, tab);
         ldh = MSM ? n : hld(n);
         // zero vector pads: the float4 pass reads columns up to hld(n)
-        for (int k = n + tid; k < nv; k += NT) { g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0); }
+        for (int k = n + tid; k < nv; k += NT) {
+            g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0);
+            if (kTwoPend && P.two_pending) { pxi2[k] = R(0); pc2[k] = R(0); }
+        }
         if (!LB) reset_matrix();
         __syncthreads();
 
@@ -976,7 +1043,8 @@ struct Opt {
         int status = MMFFB_ST_MAXIT;
         int it = 0, done_iters = 0, nevals = 0, restarts = 0;
         bool fresh = true;     // direction is -g (start or just after a restart)
-        bool pending = false;
+        int npend = 0;         // rank-2 updates not yet stored in H (at most 2, else 1)
+        const bool two_pend = kTwoPend && P.two_pending;
         int hcount = 0, hidx = 0;
         if (!isfinite((double)E) || !isfinite((double)gs_[0])) {
             status = MMFFB_ST_NONFINITE;
@@ -1015,7 +1083,7 @@ struct Opt {
                         // uphill quasi-Newton direction: restart from steepest descent
                         ++restarts;
                         fresh = true;
-                        pending = false;
+                        npend = 0;
                         hcount = 0;
                         hidx = 0;
                         reset_matrix();
@@ -1083,7 +1151,7 @@ struct Opt {
                         // no decrease along the quasi-Newton direction: restart from -g
                         ++restarts;
                         fresh = true;
-                        pending = false;
+                        npend = 0;
                         hcount = 0;
                         hidx = 0;
                         reset_matrix();
@@ -1153,9 +1221,11 @@ struct Opt {
                 }
                 if (!LB) {
                     __syncthreads();
-                    if constexpr (!MSM && NC == 0 && sizeof(R) == 4) hpass_stream_v4(pending);
-                    else if (MSM) hpass(pending);
-                    else hpass_stream(pending);
+                    const bool store = two_pend ? npend == 2 : npend > 0;
+                    if constexpr (kTwoPend) hpass_stream_v4(npend, store);
+                    else if (MSM) hpass(npend > 0);
+                    else hpass_stream(npend > 0);
+                    if (store) npend = 0;
                     __syncthreads();
                     if (!MSM && *(volatile int *)abort_flag) { status = MMFFB_ST_TIMEOUT; break; }
                     A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};
@@ -1175,17 +1245,18 @@ struct Opt {
                         const A al = fi * (A(1) + fae * fi);
                         const R cxg = (R)(al * d6[4]), cqg = (R)(fi * d6[5]), fxg = (R)(fi * d6[4]);
                         const R rfi = (R)fi, ral = (R)al;
+                        // the update joins the pending ones (the first or the second slot)
+                        R *ux = npend == 0 ? pxi : pxi2, *uc = npend == 0 ? pc : pc2, *ur = npend == 0 ? pr : pr2;
                         for (int k = tid; k < n; k += NT) {
                             const R xk = xo[k], qk = hq[k];
                             dir[k] = -(hp[k] + cxg * xk - cqg * xk - fxg * qk);
-                            pxi[k] = xk;
-                            pc[k] = -rfi * qk;
-                            pr[k] = ral * xk - rfi * qk;
+                            ux[k] = xk;
+                            uc[k] = -rfi * qk;
+                            ur[k] = ral * xk - rfi * qk;
                         }
-                        pending = true;
+                        ++npend;
                     } else {
                         for (int k = tid; k < n; k += NT) dir[k] = -hp[k];
-                        pending = false;
                     }
                 } else {
                     // L-BFGS history update (lbfgs_tg.metal:247-262)
@@ -1236,13 +1307,19 @@ __global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_k
     }
     __syncthreads();
     const int *order = P.c.order;
+    const bool queue = P.q_tail != nullptr;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
+        if (threadIdx.x == 0) s_item = queue ? claim_slot(P) : atomicAdd(P.counter, 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
-        if (item >= P.c.n_conf) break;
-        opt.run(order ? order[item] : item);
+        if (item < 0 || item >= P.c.n_conf) break;
+        opt.run(queue || !order ? item : order[item]);
+        if (queue && threadIdx.x == 0) {
+            // the slot's results are written (run() ends with a barrier): flag it for the host
+            __threadfence_system();
+            *(volatile int *)&P.q_done[item] = 1;
+        }
         // a copy never completed: stop taking work (the conformers left keep the
         // MMFFB_ST_TIMEOUT that prepare_minimize gave them; healthy CTAs go on)
         if (*(volatile int *)&s_abort) break;
@@ -1337,6 +1414,7 @@ __global__ void __launch_bounds__(NT) check64_kernel(const Params P, const doubl
 struct Plan {
     int nt, nc;
     bool msm;
+    bool two_pend;     // streamed FP32 H with two pending updates (stored every other iteration)
     size_t smem;
     int grid;
     size_t gslot;      // matrix elements per CTA slot when not in shared memory

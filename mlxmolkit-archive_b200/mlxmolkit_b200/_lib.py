@@ -40,7 +40,8 @@ class MMFFOptParams(ctypes.Structure):
                 ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
                 ("atom_grad_scale", ctypes.c_float), ("max_restarts", ctypes.c_int32),
                 ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32),
-                ("wait_spins", ctypes.c_uint32), ("err_word", P)]
+                ("wait_spins", ctypes.c_uint32), ("give_up_waits", ctypes.c_int32),
+                ("two_pending", ctypes.c_int32), ("err_word", P)]
 
 
 # (MMFFTermsHost field, MMFFParams field, ctypes element type) in the header's order
@@ -77,6 +78,11 @@ class MMFFTermsHost(ctypes.Structure):
 class MMFFPackSizes(ctypes.Structure):
     _fields_ = [("bonded_rows", ctypes.c_int64), ("atoms", ctypes.c_int64), ("cls_pairs", ctypes.c_int64),
                 ("mask_words", ctypes.c_int64)]
+
+
+class MMFFQueueDev(ctypes.Structure):
+    _fields_ = [("head", P), ("tail", P), ("close", P), ("done", P), ("idle_polls", ctypes.c_uint32),
+                ("sleep_ns", ctypes.c_uint32)]
 
 
 class MMFFMultiMolState(ctypes.Structure):
@@ -119,7 +125,8 @@ DG_CONVERGED, DG_MAXIT = 0, 1
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_fp64_check", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc", "mmffb_pack_chunk", "mmffb_pack_begin", "mmffb_pack_finish", "mmffb_pack_free",
+           "mmffb_minimize_noalloc", "mmffb_queue_scratch_bytes", "mmffb_minimize_queue",
+           "mmffb_host_alloc_mapped", "mmffb_host_free", "mmffb_pack_chunk", "mmffb_pack_begin", "mmffb_pack_finish", "mmffb_pack_free",
            "mmffb_multimol_hist_floats", "mmffb_multimol_step",
            "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad",
            "mmffb_etk_scratch_bytes", "mmffb_etk_minimize", "mmffb_etk_energy_grad", "mmffb_stereo_check"]
@@ -186,10 +193,45 @@ def load():
     L.mmffb_etk_energy_grad.argtypes = [DBP, ETP, DPP, P, P, P, P]
     L.mmffb_stereo_check.restype = ctypes.c_int
     L.mmffb_stereo_check.argtypes = [DBP, P, P, ctypes.c_float, P, P, P]
+    L.mmffb_host_alloc_mapped.restype = ctypes.c_int
+    L.mmffb_host_alloc_mapped.argtypes = [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p)]
+    L.mmffb_host_free.restype = ctypes.c_int
+    L.mmffb_host_free.argtypes = [P]
+    L.mmffb_queue_scratch_bytes.restype = ctypes.c_size_t
+    L.mmffb_queue_scratch_bytes.argtypes = [BP, CP, OP, ctypes.c_int32]
+    L.mmffb_minimize_queue.restype = ctypes.c_int
+    L.mmffb_minimize_queue.argtypes = [BP, CP, OP, ctypes.POINTER(MMFFQueueDev), P, P, P, P, ctypes.c_int32, P,
+                                       ctypes.c_size_t, P]
     L.mmffb_minimize_noalloc.restype = ctypes.c_int
     L.mmffb_minimize_noalloc.argtypes = [BP, CP, OP, P, P, P, P, P, P]
     _lib = L
     return L
+
+
+class MappedHostArray:
+    """A zeroed numpy array in host memory that the device can write (mmffb_host_alloc_mapped);
+    ``device_ptr`` is its device address.  Freed with the object."""
+
+    def __init__(self, n: int, dtype):
+        import numpy as np
+        L = load()
+        self.dtype = np.dtype(dtype)
+        host, dev = ctypes.c_void_p(), ctypes.c_void_p()
+        check(L.mmffb_host_alloc_mapped(max(1, n) * self.dtype.itemsize, ctypes.byref(host), ctypes.byref(dev)),
+              "mmffb_host_alloc_mapped")
+        self._host = host.value
+        self.device_ptr = dev.value
+        buf = (ctypes.c_char * (max(1, n) * self.dtype.itemsize)).from_address(self._host)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=max(1, n))
+
+    def __del__(self):
+        if getattr(self, "_host", None):
+            try:
+                load().mmffb_host_free(self._host)
+            except Exception:
+                pass
+            self._host = None
 
 
 def check(rc: int, what: str) -> None:

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
@@ -73,6 +74,8 @@ class DeviceBatch:
         self.cls_tab = t(packed.cls_tab.reshape(-1))
         self.pair_mask = t(packed.pair_mask.view(np.int32))
         self.n_atoms = packed.n_atoms
+        self.nbytes = sum(x.numel() * x.element_size() for x in (self.mol_desc, self.bonded, self.atom_cls,
+                                                                  self.atom_q, self.cls_tab, self.pair_mask))
 
     @classmethod
     def from_params(cls, params_list, device=None) -> "DeviceBatch":
@@ -98,6 +101,7 @@ class DeviceConformers:
         self.conf_mol = torch.from_numpy(self.conf_mol_np.copy()).to(dev)
         self.conf_coord = torch.from_numpy(np.asarray(conf_coord, dtype=np.int64).copy()).to(dev)
         self.order = None if order is None else torch.from_numpy(np.asarray(order, np.int32).copy()).to(dev)
+        self.nbytes = 12 * self.n_conf + (0 if order is None else 4 * len(order))
 
     def desc(self) -> _lib.MMFFConfDev:
         return _lib.MMFFConfDev(self.n_conf, self.max_atoms, self.conf_mol.data_ptr(),
@@ -109,13 +113,18 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
                polish64: Optional[bool] = None, hpass_lean: bool = True, wait_spins: int = 0,
-               err_word: int = 0) -> _lib.MMFFOptParams:
+               err_word: int = 0, two_pending: bool = True, give_up_waits: bool = False) -> _lib.MMFFOptParams:
     """Launch options; ``polish64`` (default: on for mixed precision) switches a conformer's
     line-search energies to FP64 once the FP32 ones stall.  ``err_word``: device address of an
     int32 that the launch sets to 1 when a bounded wait gives up; ``wait_spins`` bounds those
-    waits (0: the library default; lowered only to exercise that path)."""
+    waits (0: the library default); ``give_up_waits`` makes every such wait give up at once (a test
+    switch that exercises the timeout path).  ``two_pending``: the
+    streamed FP32 inverse Hessian is stored every other iteration where that keeps the occupancy
+    (same results)."""
     o = _lib.MMFFOptParams()
     o.wait_spins = int(wait_spins)
+    o.give_up_waits = int(bool(give_up_waits))
+    o.two_pending = 0 if two_pending else -1
     o.err_word = int(err_word) or None
     o.max_restarts = int(max_restarts)
     o.polish64 = int(precision == "mixed" if polish64 is None else bool(polish64))
@@ -152,6 +161,7 @@ class MinimizeResult:
     energies_fp64: Optional[np.ndarray] = None
     energy_errors: Optional[np.ndarray] = None
     grad_rms_fp64: Optional[np.ndarray] = None
+    timings: Optional[dict] = None     # host seconds of the drop-in call's steps (mmff_minimize_nk)
 
     @property
     def converged(self) -> np.ndarray:
@@ -168,13 +178,20 @@ class Minimizer:
             raise ValueError("give the molecules' parameters or their packed tables")
         self.params_list = list(params_list) if params_list is not None else None
         self.conf_counts = [int(k) for k in conf_counts]
-        self.batch = DeviceBatch(packed, device) if packed is not None else \
-            DeviceBatch.from_params(self.params_list, device)
-        n_atoms = [int(v) for v in packed.n_atoms] if packed is not None else [int(p.n_atoms) for p in self.params_list]
+        t = time.perf_counter()
+        if packed is None:
+            packed = pack_molecules(self.params_list)
+            self.pack_s = time.perf_counter() - t
+        else:
+            self.pack_s = 0.0
+        self.batch = DeviceBatch(packed, device)
+        n_atoms = [int(v) for v in packed.n_atoms]
         self.conf_mol, self.conf_coord, self.total = conformer_index(n_atoms, self.conf_counts)
         self.order = lpt_order(n_atoms, self.conf_mol)
         self.confs = DeviceConformers(self.batch, self.conf_mol, self.conf_coord, self.order)
         self._scratch = None
+        # host -> device bytes of the set-up (tables and conformer index arrays)
+        self.upload_bytes = self.batch.nbytes + self.confs.nbytes
 
     def _scratch_for(self, nbytes: int):
         torch = _torch()
@@ -187,7 +204,7 @@ class Minimizer:
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
                         hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
-                        wait_spins: int = 0):
+                        wait_spins: int = 0, two_pending: bool = True, give_up_waits: bool = False):
         """Minimise in place on the device; returns (energy, status, iters) device tensors.
 
         ``evals`` (optional int32 device tensor, one per conformer) receives the
@@ -206,7 +223,7 @@ class Minimizer:
             e, st, it = out
         o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode, threads, ctas_per_sm,
                        exit_test, check_every, atom_grad_scale, max_restarts, polish64, hpass_lean,
-                       wait_spins, err.data_ptr() if err is not None else 0)
+                       wait_spins, err.data_ptr() if err is not None else 0, two_pending, give_up_waits)
         bd, cd = self.batch.desc(), self.confs.desc()
         nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
         if nbytes == 0 and C > 0:
@@ -341,7 +358,7 @@ class BinnedMinimizer(Minimizer):
     def __init__(self, params_list, conf_counts, device=None, bins=DEFAULT_BINS, tuning=None):
         super().__init__(params_list, conf_counts, device)
         torch = _torch()
-        n_atoms = np.array([int(p.n_atoms) for p in self.params_list], dtype=np.int64)
+        n_atoms = np.asarray(self.batch.n_atoms, dtype=np.int64)
         nconf = n_atoms[self.conf_mol]
         self.bins = []
         self._bin_events = []
@@ -354,6 +371,7 @@ class BinnedMinimizer(Minimizer):
                 dc.n_conf = len(order)          # the bin's queue: its own order array
                 dc.max_atoms = int(nconf[sel].max())
                 cfg = dict((tuning or {}).get(str(hi), (tuning or {}).get(hi, {})))
+                self.upload_bytes += dc.nbytes
                 self.bins.append({"hi": hi, "confs": dc, "n": len(order), "cfg": cfg, "sel": sel,
                                   "stream": torch.cuda.Stream(device=self.batch.device), "scratch": None,
                                   "cost": float(np.sum((3.0 * nconf[sel]) ** 2))})
@@ -367,7 +385,8 @@ class BinnedMinimizer(Minimizer):
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
                         hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
-                        wait_spins: int = 0, time_bins=False):
+                        wait_spins: int = 0, two_pending: bool = True, give_up_waits: bool = False,
+                        time_bins=False):
         """As ``Minimizer.minimize_device``, one launch per size class.  With
         ``time_bins`` each launch is bracketed by timing events on its own stream;
         ``bin_times_ms()`` reads them after a synchronize."""
@@ -390,7 +409,7 @@ class BinnedMinimizer(Minimizer):
             o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode,
                            threads or cfg.get("threads", 0), ctas_per_sm or cfg.get("ctas_per_sm", 0),
                            exit_test, check_every, atom_grad_scale, max_restarts, polish64,
-                           bool(cfg.get("lean", hpass_lean)), wait_spins, 0)
+                           bool(cfg.get("lean", hpass_lean)), wait_spins, 0, two_pending, give_up_waits)
             cd = b["confs"].desc()
             nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
             if b["scratch"] is None or b["scratch"].numel() < nbytes:
@@ -434,16 +453,29 @@ def mmff_minimize_nk(
     max_iters: int = 500,
     grad_tol: float = 1e-4,
     use_lbfgs: bool = False,
-) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
-    """Minimise N molecules x k conformers on the GPU (one persistent launch).
+    return_result: bool = False,
+):
+    """Minimise N molecules x k conformers on the GPU (one persistent launch per size class).
 
     Same signature and return values as the reference
     (mlxmolkit/mmff_minimize.py:231-346): ``positions_3d`` is the flat
     float32 coordinate array of all conformers, molecule-major; returns
     (positions float32 flat, energies float32 (C,), converged bool (C,)).
     ``use_lbfgs`` selects L-BFGS with 8 history pairs instead of dense BFGS.
+    Like the reference, every call packs the molecules' tables (here on host
+    threads, natively) and uploads them.  With ``return_result`` a fourth item,
+    the ``MinimizeResult``, carries each conformer's status, iterations and FP64
+    check (FP64 energy at the returned coordinates, the returned energy's error
+    against it, FP64 RMS gradient) and the host time of each step.
     """
+    t0 = time.perf_counter()
     m = BinnedMinimizer(mmff_params_list, conf_counts, tuning=load_tuning())
+    t1 = time.perf_counter()
     r = m.minimize(positions_3d, max_iters=max_iters, grad_tol=grad_tol,
                    history_m=LBFGS_M if use_lbfgs else 0)
-    return r.positions, r.energies.astype(np.float32), r.converged
+    t2 = time.perf_counter()
+    if not return_result:
+        return r.positions, r.energies.astype(np.float32), r.converged
+    r.timings = {"setup_s": t1 - t0, "pack_s": m.pack_s, "minimize_s": t2 - t1, "total_s": t2 - t0,
+                 "upload_bytes": int(m.upload_bytes)}
+    return r.positions, r.energies.astype(np.float32), r.converged, r

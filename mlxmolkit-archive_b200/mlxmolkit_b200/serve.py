@@ -1,27 +1,37 @@
-"""Continuous-batching MMFF optimisation service on one GPU.
+"""Continuous-batching MMFF optimisation service on one GPU, with slot-level admission.
 
 Requests (one molecule x k conformers, MMFF94 or MMFF94s) arrive at any
 time.  The service
 
 * prepares each request on the host in a small thread pool, overlapping the
-  GPU: term extraction and packing of the molecule's device tables, cached
-  per molecular graph and MMFF variant (repeat molecules skip both);
-* sorts prepared requests into size classes (below).  Whenever a CUDA stream
-  is free and the device-memory budget allows, it launches all the waiting
-  requests of a class, up to a conformer cap, as ONE persistent optimizer
-  launch.  Requests that arrive while others are on the GPU therefore join
-  the next launch of their class, and launches of different classes and
-  successive launches overlap on separate streams;
-* keeps a launch's coordinates, tables, optimizer scratch and results
-  resident on the device until the kernel ends.  The tables, coordinates and
-  results go through pinned staging buffers owned by the stream and reused
-  from launch to launch.  The service then completes each request's future.
+  GPU: term extraction and native packing of the molecule's device tables,
+  cached per molecular graph and MMFF variant (repeat molecules skip both);
+* keeps, per size class, a device arena in two halves and a persistent
+  worker launch (``mmffb_minimize_queue``) that takes conformer slots from a
+  device work queue while it runs.  A prepared request is copied into the
+  open half of its class -- tables, slot descriptors, coordinates -- on the
+  class's copy stream, followed by the queue's new tail, so the running
+  worker's CTAs pick its conformers up as soon as they finish their current
+  ones: a request admitted while others are on the GPU joins the running
+  launch instead of waiting for the next one;
+* learns that a slot is finished from a flag the kernel writes to mapped host
+  memory, copies each finished request's results back and completes its
+  future.
+
+A worker whose queue stays empty for 10 ms ends (every wait in the kernel is
+bounded) and frees its SMs for the other classes; new slots start a new
+launch when the newest one is older than that, and several launches may share
+a queue.  A half is filled in order and refilled only when its worker
+launches have ended and its requests are complete, so no running launch ever
+reads memory written after it started; the other half takes the requests
+meanwhile.  Device memory is bounded by the budget: arenas and worker scratch
+per size class.
 
 Size classes fix the kernel instance: each class launches with a fixed atom
 bound and class-table size, so the instance (CTA size, Hessian in shared
 memory or in a global slot, dense BFGS or L-BFGS) depends on the class only.
-The kernel's result for a conformer depends only on the instance (work is
-pulled from a queue and no value crosses conformers), so a request's result
+The kernel's result for a conformer depends only on the instance (slots are
+claimed from a queue and no value crosses conformers), so a request's result
 is bit-for-bit the same alone or in any mix of requests.
 
 | atoms   | optimizer   | atom bound | class-table bound |
@@ -156,81 +166,184 @@ def topology_key(mol, variant: str):
     return (variant, atoms, bonds, types)
 
 
-class _Staging:
-    """Pinned host and device byte buffers of one stream, grown on demand and reused."""
+@dataclass
+class _Caps:
+    """Capacity of one half of a size class's device arena."""
+    slots: int
+    coords: int
+    mols: int
+    rows: int
+    atoms: int
+    pairs: int
+    words: int
 
-    def __init__(self, torch, device):
-        self.torch = torch
-        self.device = device
-        self.host: dict = {}
-        self.dev: dict = {}
-
-    def _get(self, store, name, nbytes, pinned):
-        torch = self.torch
-        b = store.get(name)
-        if b is None or b.numel() < nbytes:
-            size = max(2 * nbytes, 1 << 16)
-            b = (torch.empty(size, dtype=torch.uint8, pin_memory=True) if pinned else
-                 torch.empty(size, dtype=torch.uint8, device=self.device))
-            store[name] = b
-        return b
-
-    def upload(self, name, arr: np.ndarray, stream):
-        """Copy a host array into this stream's device buffer `name` (async, through pinned memory)."""
-        a = np.ascontiguousarray(arr)
-        nb = max(a.nbytes, 16)
-        h = self._get(self.host, name, nb, True)
-        h.numpy()[:a.nbytes] = a.reshape(-1).view(np.uint8)
-        d = self._get(self.dev, name, nb, False)
-        with self.torch.cuda.stream(stream):
-            d[:a.nbytes].copy_(h[:a.nbytes], non_blocking=True)
-        return d
-
-    def device_buf(self, name, nbytes):
-        return self._get(self.dev, name, max(nbytes, 16), False)
-
-    def download(self, name, dev_buf, nbytes, stream):
-        """Queue a device -> pinned host copy; returns the host buffer (valid after the stream syncs)."""
-        h = self._get(self.host, name, max(nbytes, 16), True)
-        with self.torch.cuda.stream(stream):
-            h[:nbytes].copy_(dev_buf[:nbytes], non_blocking=True)
-        return h
+    def nbytes(self) -> int:
+        return (self.slots * (4 + 8 + 8 + 4 + 4) + self.coords * 4 + self.mols * 64 + self.rows * 16
+                + self.atoms * 12 + self.pairs * 8 + self.words * 4 + 16)
 
 
-class _Launch:
-    def __init__(self, reqs, cls, stream_idx, event, out, nbytes):
-        self.reqs = reqs
+def arena_caps(cls: SizeClass, half_bytes: int, max_slots: int = 4096) -> Optional[_Caps]:
+    """The largest half arena of class ``cls`` within ``half_bytes`` (None if not even 2 slots fit).
+
+    Tables are provisioned for one molecule per two conformer slots, each molecule at the
+    class's atom bound: 40 bonded records and 12 B per atom, the class table and the bit rows.
+    """
+    n = cls.nmax
+    w = (n + 31) // 32
+
+    def caps(slots):
+        mols = max(1, slots // 2)
+        return _Caps(slots, slots * 3 * n, mols, mols * 40 * n, mols * n, mols * cls.max_classes ** 2,
+                     mols * 2 * n * w)
+    slots = max_slots
+    while slots >= 2 and caps(slots).nbytes() > half_bytes:
+        slots //= 2
+    return caps(slots) if slots >= 2 else None
+
+
+class _Half:
+    """One half of a size class's device arena: the tables, conformer slots and results of the
+    requests one worker generation serves.  Addresses are handed out in order (bump pointers)
+    and the half is refilled only after its worker ended, so no running launch reads memory
+    written after it started."""
+
+    def __init__(self, srv, caps: _Caps):
+        torch = srv.torch
+        dev = srv.device
+        z = lambda n, dt: torch.zeros(max(int(n), 1), dtype=dt, device=dev)
+        self.caps = caps
+        self.mol_desc = z(16 * caps.mols, torch.int32)
+        self.bonded = z(4 * caps.rows, torch.int32)
+        self.atom_cls = z(caps.atoms, torch.int32)
+        self.atom_q = z(caps.atoms, torch.float64)
+        self.cls_tab = z(2 * caps.pairs, torch.float32)
+        self.pair_mask = z(caps.words, torch.int32)
+        self.conf_mol = z(caps.slots, torch.int32)
+        self.conf_coord = z(caps.slots, torch.int64)
+        self.pos = z(caps.coords, torch.float32)
+        self.energy = z(caps.slots, torch.float64)
+        self.status = z(caps.slots, torch.int32)
+        self.iters = z(caps.slots, torch.int32)
+        self.ctl = z(4, torch.int32)              # head, tail (published slots), close
+        self.done_buf = _lib.MappedHostArray(caps.slots, np.int32)   # per-slot "results written" flags
+        self.done_np = self.done_buf.array
+        self.done_dev = self.done_buf.device_ptr
+        self.workers: list = []                   # (end event, scratch index, launch time) of its launches
+        self.closed = True
+        self.requests: list = []
+        self.n_mol = self.n_row = self.n_atom = self.n_pair = self.n_word = self.n_slot = self.n_coord = 0
+
+    def start(self, stream) -> None:
+        """Empty the half for a new generation (no worker of it may be running)."""
+        import torch
+        self.n_mol = self.n_row = self.n_atom = self.n_pair = self.n_word = self.n_slot = self.n_coord = 0
+        self.done_np[:] = 0
+        with torch.cuda.stream(stream):
+            self.ctl.zero_()
+        self.closed = False
+        self.requests = []
+
+    def fits(self, pk, k: int, n_atoms: int) -> bool:
+        return _fits(self, self.caps, pk, k, n_atoms)
+
+    def reserve(self, r) -> None:
+        """Hand the request its molecule, records, atoms, class table, bit rows, slots and
+        coordinates (in order, so a tick's requests are contiguous)."""
+        pk, k, n = r.packed, r.positions.shape[0], int(r.params.n_atoms)
+        r.half = self
+        r.base = (self.n_mol, self.n_row, self.n_atom, self.n_pair, self.n_word, self.n_slot, self.n_coord)
+        r.slot0, r.coord0 = self.n_slot, self.n_coord
+        self.n_mol += 1
+        self.n_row += len(pk.bonded)
+        self.n_atom += len(pk.atom_cls)
+        self.n_pair += len(pk.cls_tab)
+        self.n_word += len(pk.pair_mask)
+        self.n_slot += k
+        self.n_coord += 3 * n * k
+        self.requests.append(r)
+
+    def live_workers(self) -> list:
+        """Launches on this half that have not ended (ended ones are dropped)."""
+        self.workers = [w for w in self.workers if not w[0].query()]
+        return self.workers
+
+    def worker_running(self) -> bool:
+        return bool(self.live_workers())
+
+    def idle(self) -> bool:
+        """Closed, no worker running and every request completed: free for a new generation."""
+        return self.closed and not self.worker_running() and not self.requests
+
+
+class _ClassState:
+    def __init__(self, srv, key, cls: SizeClass, max_iters: int, caps: _Caps):
+        torch = srv.torch
+        self.key = key
         self.cls = cls
-        self.stream_idx = stream_idx
-        self.event = event
-        self.out = out             # (pos host, E host, status host, iters host, offsets)
-        self.nbytes = nbytes
+        self.max_iters = max_iters
+        self.halves = [_Half(srv, caps), _Half(srv, caps)]
+        self.cur = None
+        self.copy_stream = torch.cuda.Stream(device=srv.device)
+        self.opt = mm.opt_params(max_iters, 1e-4, cls.history_m, "mixed")
+        h = self.halves[0]
+        bd, cd = self._descs(h)
+        need = srv.lib.mmffb_queue_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(self.opt), 0)
+        if need == 0:
+            _lib.check(_lib.MMFFB_EINVAL, "mmffb_queue_scratch_bytes")
+        # each concurrent worker launch needs its own scratch (work counter, error word, inverse-
+        # Hessian slots per CTA): up to MAX_WORKERS launches of the class at once, as a quarter
+        # of the budget allows
+        nw = int(max(1, min(self.MAX_WORKERS, (srv.budget // 4) // max(need, 1))))
+        self.scratch = [torch.empty(need, dtype=torch.uint8, device=srv.device) for _ in range(nw)]
+        self.scratch_busy = [None] * nw                # end event of the launch using it
+        self.compute_streams = [torch.cuda.Stream(device=srv.device) for _ in range(nw)]
+        self.nbytes = 2 * caps.nbytes() + nw * need
+        self.launches = 0
+
+    MAX_WORKERS = 4
+
+    def free_scratch(self) -> Optional[int]:
+        for i, ev in enumerate(self.scratch_busy):
+            if ev is None or ev.query():
+                self.scratch_busy[i] = None
+                return i
+        return None
+
+    def _descs(self, h: _Half):
+        c = h.caps
+        bd = _lib.MMFFBatchDev(c.mols, self.cls.nmax, self.cls.max_classes, h.mol_desc.data_ptr(),
+                               h.bonded.data_ptr(), h.atom_cls.data_ptr(), h.atom_q.data_ptr(),
+                               h.cls_tab.data_ptr(), h.pair_mask.data_ptr())
+        cd = _lib.MMFFConfDev(c.slots, self.cls.nmax, h.conf_mol.data_ptr(), h.conf_coord.data_ptr(), 0)
+        return bd, cd
 
 
 class MMFFServer:
-    """Admission-by-budget continuous batching: one launch per size class and free stream."""
+    """Continuous batching with slot-level admission: one persistent worker per size class takes
+    conformer slots from a device work queue while it runs."""
 
-    def __init__(self, hbm_budget_bytes: int = 8 << 30, n_streams: int = 8, prep_workers: int = 4,
-                 device=None, default_max_iters: int = 1000, default_max_iters_lbfgs: int = 3000,
-                 max_launch_conformers: int = 4096,
-                 prep_cache_size: int = 4096):
+    SLEEP_NS = 20000          # pause between a worker's polls of an empty queue
+
+    def __init__(self, hbm_budget_bytes: int = 8 << 30, prep_workers: int = 4, device=None,
+                 default_max_iters: int = 1000, default_max_iters_lbfgs: int = 3000,
+                 max_slots_per_half: int = 4096, prep_cache_size: int = 4096, worker_idle_ms: float = 10.0):
+        """``worker_idle_ms``: a worker launch whose queue stays empty this long ends."""
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("MMFFServer needs a CUDA device")
+        self.IDLE_POLLS = max(1, int(worker_idle_ms * 1e6 / self.SLEEP_NS))
         self.torch = torch
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         self.budget = int(hbm_budget_bytes)
         self.in_use = 0
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
-        self.staging = [_Staging(torch, self.device) for _ in range(n_streams)]
-        self.free_streams = list(range(n_streams))
         self.default_max_iters = default_max_iters
         self.default_max_iters_lbfgs = default_max_iters_lbfgs
-        self.max_launch_conformers = int(max_launch_conformers)
+        self.max_slots_per_half = int(max_slots_per_half)
         self.pool = ThreadPoolExecutor(max_workers=prep_workers)
         self.incoming: "queue.Queue[_Req]" = queue.Queue()
         self.waiting: list[_Req] = []
-        self.running: list[_Launch] = []
+        self.copying: list = []               # (request, event, host results)
+        self.classes: dict = {}
         self.next_id = 0
         self.lock = threading.Lock()
         self.stop_flag = threading.Event()
@@ -241,6 +354,7 @@ class MMFFServer:
         self.prep_cache_size = int(prep_cache_size)
         self.prep_hits = 0
         self.lib = _lib.load()
+        self.error: Optional[BaseException] = None
         self.thread = threading.Thread(target=self._loop, name="mmff-server", daemon=True)
         self.thread.start()
 
@@ -298,80 +412,170 @@ class MMFFServer:
         return r
 
     # --- scheduler side ---
-    def _launch(self, reqs, cls: SizeClass, sidx: int, nbytes: int) -> None:
+    def _class_state(self, r: _Req) -> Optional[_ClassState]:
+        key = (r.cls, r.max_iters)
+        cs = self.classes.get(key)
+        if cs is None:
+            caps = arena_caps(r.cls, max(self.budget // 12, 0), self.max_slots_per_half)
+            if caps is None:
+                raise MemoryError(f"request {r.rid}: the {self.budget} B budget holds no arena for its size class")
+            cs = _ClassState(self, key, r.cls, r.max_iters, caps)
+            if self.in_use + cs.nbytes > self.budget:
+                raise MemoryError(f"request {r.rid}: size class {r.cls.key} needs {cs.nbytes} B of arenas, "
+                                  f"{self.budget - self.in_use} B of the budget are left")
+            self.in_use += cs.nbytes
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
+            self.classes[key] = cs
+        return cs
+
+    def _half_for(self, cs: _ClassState, r: _Req, to_close: list) -> Optional[_Half]:
+        """The open half that takes r, switching generations when the current one is full (the
+        full half is closed after this tick's slots are published)."""
+        k, n = r.positions.shape[0], int(r.params.n_atoms)
+        if not _fits(_EmptyHalf(), cs.halves[0].caps, r.packed, k, n):
+            raise MemoryError(f"request {r.rid} ({k} conformers of {n} atoms) exceeds its size class's arena")
+        h = cs.cur
+        if h is not None and not h.closed and h.fits(r.packed, k, n):
+            return h
+        other = cs.halves[1] if h is cs.halves[0] else cs.halves[0]
+        if not other.idle():
+            return None                       # both halves busy: r waits
+        if h is not None and not h.closed:
+            h.closed = True
+            to_close.append((cs, h))
+        other.start(cs.copy_stream)
+        cs.cur = other
+        return other
+
+    def _close_half(self, cs: _ClassState, h: _Half) -> None:
+        """No more slots: the worker ends once it has claimed every published one."""
+        torch = self.torch
+        with torch.cuda.stream(cs.copy_stream):
+            h.ctl[2:3].copy_(torch.ones(1, dtype=torch.int32).pin_memory(), non_blocking=True)
+        h.closed = True
+
+    def _publish(self, cs: _ClassState, h: _Half, reqs) -> None:
+        """Copy the requests' tables, slot descriptors and coordinates into their reserved, contiguous
+        places in the half, then the new tail (ordered after them on the copy stream), and start a
+        worker if none is running."""
+        torch = self.torch
+        pk = merge_packed([r.packed for r in reqs])
+        m0, row0, atom0, pair0, word0, slot0, coord0 = reqs[0].base
+        desc = pk.mol_desc.copy()
+        desc[:, MD_ATOM_OFF] += atom0
+        desc[:, MD_CLS_OFF] += pair0
+        desc[:, MD_MASK_OFF] += word0
+        for t in range(5):
+            desc[:, MD_B_OFF + 2 * t] += row0
+        counts = [r.positions.shape[0] for r in reqs]
+        conf_mol = (np.repeat(np.arange(len(reqs)), counts) + m0).astype(np.int32)
+        sizes = np.repeat(3 * pk.n_atoms.astype(np.int64), counts)
+        coord = coord0 + np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        pos = np.concatenate([r.positions.reshape(-1) for r in reqs]).astype(np.float32)
+        t_admit = time.perf_counter()
+        for r in reqs:
+            r.t_admit = t_admit
+
+        def put(dst, start, arr, dtype):
+            a = torch.from_numpy(np.ascontiguousarray(arr).reshape(-1).view(dtype)).pin_memory()
+            dst[start:start + a.numel()].copy_(a, non_blocking=True)
+
+        with torch.cuda.stream(cs.copy_stream):
+            put(h.mol_desc, 16 * m0, desc, np.int32)
+            put(h.bonded, 4 * row0, pk.bonded, np.int32)
+            put(h.atom_cls, atom0, pk.atom_cls, np.int32)
+            put(h.atom_q, atom0, pk.atom_q, np.float64)
+            put(h.cls_tab, 2 * pair0, pk.cls_tab, np.float32)
+            put(h.pair_mask, word0, pk.pair_mask, np.int32)
+            put(h.conf_mol, slot0, conf_mol, np.int32)
+            put(h.conf_coord, slot0, coord, np.int64)
+            put(h.pos, coord0, pos, np.float32)
+            put(h.ctl, 1, np.array([slot0 + len(conf_mol)], np.int32), np.int32)     # the new tail
+            ready = torch.cuda.Event()
+            ready.record(cs.copy_stream)
+        self._ensure_worker(cs, h, ready)
+
+    def _ensure_worker(self, cs: _ClassState, h: _Half, ready) -> None:
+        """Start a worker on h unless a recent one runs: a worker older than its idle limit may
+        have lost the CTAs that found the queue empty, so new slots get a fresh launch whose CTAs
+        take SMs as they free up (concurrent launches share the queue)."""
+        live = h.live_workers()
+        idle_s = self.IDLE_POLLS * self.SLEEP_NS * 1e-9
+        if live and time.perf_counter() - max(w[2] for w in live) < idle_s:
+            return
+        i = cs.free_scratch()
+        if i is None:
+            return                          # every scratch is in use: the running launches take the slots
+        self._launch_worker(cs, h, ready, i)
+
+    def _launch_worker(self, cs: _ClassState, h: _Half, ready, i: int) -> None:
         torch = self.torch
         L = self.lib
-        stream = self.streams[sidx]
-        stg = self.staging[sidx]
-        pk = merge_packed([r.packed for r in reqs])
-        counts = [r.positions.shape[0] for r in reqs]
-        n_atoms = pk.n_atoms.astype(np.int64)
-        conf_mol, coord, total = conformer_index(n_atoms, counts)
-        order = lpt_order(n_atoms, conf_mol)
-        pos = np.concatenate([r.positions.reshape(-1) for r in reqs]).astype(np.float32)
-        C = len(conf_mol)
-        d_desc = stg.upload("mol_desc", pk.mol_desc.reshape(-1), stream)
-        d_bond = stg.upload("bonded", pk.bonded.reshape(-1), stream)
-        d_cls = stg.upload("atom_cls", pk.atom_cls, stream)
-        d_q = stg.upload("atom_q", pk.atom_q, stream)
-        d_tab = stg.upload("cls_tab", pk.cls_tab.reshape(-1), stream)
-        d_mask = stg.upload("pair_mask", pk.pair_mask, stream)
-        d_cm = stg.upload("conf_mol", conf_mol.astype(np.int32), stream)
-        d_co = stg.upload("conf_coord", coord.astype(np.int64), stream)
-        d_or = stg.upload("order", order.astype(np.int32), stream)
-        d_pos = stg.upload("pos", pos, stream)
-        d_e = stg.device_buf("energy", 8 * C)
-        d_st = stg.device_buf("status", 4 * C)
-        d_it = stg.device_buf("iters", 4 * C)
-        bd = _lib.MMFFBatchDev(pk.n_mols, cls.nmax, cls.max_classes, d_desc.data_ptr(), d_bond.data_ptr(),
-                               d_cls.data_ptr(), d_q.data_ptr(), d_tab.data_ptr(), d_mask.data_ptr())
-        cd = _lib.MMFFConfDev(C, cls.nmax, d_cm.data_ptr(), d_co.data_ptr(), d_or.data_ptr())
-        o = mm.opt_params(reqs[0].max_iters, 1e-4, cls.history_m, "mixed")
-        need = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
-        if need == 0:
-            _lib.check(_lib.MMFFB_EINVAL, "mmffb_minimize_scratch_bytes")
-        scratch = stg.device_buf("scratch", need)
-        rc = L.mmffb_minimize(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o), d_pos.data_ptr(),
-                              d_e.data_ptr(), d_st.data_ptr(), d_it.data_ptr(), None, scratch.data_ptr(),
-                              scratch.numel(), ctypes.c_void_p(stream.cuda_stream))
-        _lib.check(rc, "mmffb_minimize")
-        h_pos = stg.download("pos_out", d_pos, 4 * total, stream)
-        h_e = stg.download("energy_out", d_e, 8 * C, stream)
-        h_st = stg.download("status_out", d_st, 4 * C, stream)
-        h_it = stg.download("iters_out", d_it, 4 * C, stream)
+        stream = cs.compute_streams[i]
+        stream.wait_event(ready)
+        bd, cd = cs._descs(h)
+        q = _lib.MMFFQueueDev(h.ctl.data_ptr(), h.ctl.data_ptr() + 4, h.ctl.data_ptr() + 8, h.done_dev,
+                              self.IDLE_POLLS, self.SLEEP_NS)
+        sc = cs.scratch[i]
+        rc = L.mmffb_minimize_queue(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(cs.opt), ctypes.byref(q),
+                                    h.pos.data_ptr(), h.energy.data_ptr(), h.status.data_ptr(),
+                                    h.iters.data_ptr(), 0, sc.data_ptr(), sc.numel(),
+                                    ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "mmffb_minimize_queue")
         ev = torch.cuda.Event()
         ev.record(stream)
-        t = time.perf_counter()
-        for r in reqs:
-            r.t_admit = t
-        starts = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        self.running.append(_Launch(reqs, cls, sidx, ev, (h_pos, h_e, h_st, h_it, starts, coord, C, total),
-                                    nbytes))
-        self.in_use += nbytes
-        self.peak_in_use = max(self.peak_in_use, self.in_use)
+        h.workers.append((ev, i, time.perf_counter()))
+        cs.scratch_busy[i] = ev
+        cs.launches += 1
         self.launches += 1
 
-    def _finish(self, ln: _Launch) -> None:
-        h_pos, h_e, h_st, h_it, starts, coord, C, total = ln.out
-        pos = np.frombuffer(h_pos.numpy(), dtype=np.float32, count=total)
-        e = np.frombuffer(h_e.numpy(), dtype=np.float64, count=C)
-        st = np.frombuffer(h_st.numpy(), dtype=np.int32, count=C)
+    def _collect(self, cs: _ClassState) -> None:
+        """Requests whose slots are all done: copy their results back (copy stream)."""
+        torch = self.torch
+        for h in cs.halves:
+            keep = []
+            for r in h.requests:
+                k, n = r.positions.shape[0], r.positions.shape[1]
+                if not h.done_np[r.slot0:r.slot0 + k].all():
+                    keep.append(r)
+                    continue
+                with torch.cuda.stream(cs.copy_stream):
+                    hp = torch.empty(3 * n * k, dtype=torch.float32).pin_memory()
+                    he = torch.empty(k, dtype=torch.float64).pin_memory()
+                    hs = torch.empty(k, dtype=torch.int32).pin_memory()
+                    hp.copy_(h.pos[r.coord0:r.coord0 + 3 * n * k], non_blocking=True)
+                    he.copy_(h.energy[r.slot0:r.slot0 + k], non_blocking=True)
+                    hs.copy_(h.status[r.slot0:r.slot0 + k], non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(cs.copy_stream)
+                self.copying.append((r, ev, hp, he, hs))
+            h.requests = keep
+            # a worker that ended on an empty queue leaves later slots unclaimed: start another
+            if keep and not h.worker_running():
+                ready = torch.cuda.Event()
+                ready.record(cs.copy_stream)
+                self._ensure_worker(cs, h, ready)
+
+    def _finish_copies(self) -> None:
+        keep = []
         t = time.perf_counter()
-        for i, r in enumerate(ln.reqs):
-            a, b = int(starts[i]), int(starts[i + 1])
+        for item in self.copying:
+            r, ev, hp, he, hs = item
+            if not ev.query():
+                keep.append(item)
+                continue
             k, n = r.positions.shape[0], r.positions.shape[1]
-            p = pos[int(coord[a]): int(coord[a]) + 3 * n * k].reshape(k, n, 3).copy()
-            s = st[a:b].copy()
-            r.future.set_result(RequestResult(r.rid, p, e[a:b].copy(), s, np.isin(s, mm.CONVERGED_STATUSES),
-                                              r.t_submit, r.t_admit, t))
+            st = hs.numpy().copy()
+            r.future.set_result(RequestResult(r.rid, hp.numpy().reshape(k, n, 3).copy(), he.numpy().copy(), st,
+                                              np.isin(st, mm.CONVERGED_STATUSES), r.t_submit, r.t_admit, t))
             self.completed += 1
-        self.in_use -= ln.nbytes
-        self.free_streams.append(ln.stream_idx)
+        self.copying = keep
 
     def _admit(self) -> None:
-        """Launch the waiting, prepared requests of each size class while streams and budget allow."""
-        ready: dict = {}
+        """Reserve and publish every prepared request in its size class's open half, in arrival order."""
         keep = []
+        groups: dict = {}
+        to_close: list = []
         for r in self.waiting:
             if not r.prep.done():
                 keep.append(r)
@@ -379,38 +583,27 @@ class MMFFServer:
             if r.prep.exception() is not None:
                 r.future.set_exception(r.prep.exception())
                 continue
-            alone = r.nbytes + launch_scratch_bytes(r.cls, r.positions.shape[0])
-            if alone > self.budget:
-                r.future.set_exception(MemoryError(
-                    f"request {r.rid} needs {alone} B, above the {self.budget} B budget"))
+            try:
+                cs = self._class_state(r)
+                h = self._half_for(cs, r, to_close)
+            except MemoryError as exc:
+                r.future.set_exception(exc)
                 continue
-            ready.setdefault((r.cls, r.max_iters), []).append(r)
-        # oldest request first across classes
-        for (cls, _), reqs in sorted(ready.items(), key=lambda kv: kv[1][0].t_submit):
-            while reqs and self.free_streams:
-                take, confs, nbytes = [], 0, 0
+            if h is None:
+                keep.append(r)
+                continue
+            h.reserve(r)
+            groups.setdefault((id(cs), id(h)), (cs, h, []))[2].append(r)
+        for cs, h, reqs in groups.values():
+            try:
+                self._publish(cs, h, reqs)
+            except Exception as exc:        # pragma: no cover - surfaced to the clients
                 for r in reqs:
-                    k = r.positions.shape[0]
-                    if take and confs + k > self.max_launch_conformers:
-                        break
-                    extra = nbytes + r.nbytes + launch_scratch_bytes(cls, confs + k)
-                    if self.in_use + extra > self.budget:
-                        break
-                    take.append(r)
-                    confs += k
-                    nbytes += r.nbytes
-                if not take:
-                    break
-                total = nbytes + launch_scratch_bytes(cls, confs)
-                sidx = self.free_streams.pop()
-                try:
-                    self._launch(take, cls, sidx, total)
-                except Exception as exc:
-                    self.free_streams.append(sidx)
-                    for r in take:
+                    if not r.future.done():
                         r.future.set_exception(exc)
-                reqs = reqs[len(take):]
-            keep.extend(reqs)
+                h.requests = [x for x in h.requests if x not in reqs]
+        for cs, h in to_close:
+            self._close_half(cs, h)
         self.waiting = keep
 
     def _loop(self) -> None:
@@ -422,22 +615,44 @@ class MMFFServer:
                     self.waiting.append(self.incoming.get_nowait())
             except queue.Empty:
                 pass
-            still = []
-            for ln in self.running:
-                if ln.event.query():
-                    try:
-                        self._finish(ln)
-                    except Exception as exc:  # pragma: no cover - surfaced to the clients
-                        for r in ln.reqs:
-                            if not r.future.done():
-                                r.future.set_exception(exc)
-                else:
-                    still.append(ln)
-            self.running = still
-            self._admit()
-            if self.stop_flag.is_set() and not self.waiting and not self.running and self.incoming.empty():
+            try:
+                for cs in list(self.classes.values()):
+                    self._collect(cs)
+                self._finish_copies()
+                self._admit()
+            except BaseException as exc:    # pragma: no cover - fail every open request
+                self.error = exc
+                for r in self.waiting:
+                    if not r.future.done():
+                        r.future.set_exception(exc)
+                self.waiting = []
+            pending = any(h.requests for cs in self.classes.values() for h in cs.halves)
+            if self.stop_flag.is_set() and not self.waiting and not pending and not self.copying \
+                    and self.incoming.empty():
+                for cs in self.classes.values():
+                    for h in cs.halves:
+                        if not h.closed:
+                            self._close_half(cs, h)
+                for cs in self.classes.values():
+                    cs.copy_stream.synchronize()
+                    for st in cs.compute_streams:
+                        st.synchronize()
                 break
             time.sleep(0.0002)
+
+
+class _EmptyHalf:
+    """Counters of an empty half (the capacity check of a request alone)."""
+
+    n_mol = n_row = n_atom = n_pair = n_word = n_slot = n_coord = 0
+
+
+def _fits(h, c: _Caps, pk, k: int, n_atoms: int) -> bool:
+    """Whether one more molecule (packed tables pk) with k conformers fits after h's counters."""
+    return (h.n_mol + 1 <= c.mols and h.n_row + len(pk.bonded) <= c.rows
+            and h.n_atom + len(pk.atom_cls) <= c.atoms and h.n_pair + len(pk.cls_tab) <= c.pairs
+            and h.n_word + len(pk.pair_mask) <= c.words and h.n_slot + k <= c.slots
+            and h.n_coord + 3 * n_atoms * k <= c.coords)
 
 
 def poisson_stream(server: MMFFServer, make_request, rate_confs_per_s: float, duration_s: float,

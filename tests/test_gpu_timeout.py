@@ -1,11 +1,11 @@
 """The bounded waits of the streamed inverse-Hessian pass, made to give up.
 
-With ``wait_spins=1`` a wait on a row copy gives up whenever its first,
-non-blocking test finds the copy still in flight -- at the start of every
-streamed pass it is.  No copy is broken: the copies finish normally and the
-kernel drains them before the CTA leaves.  The test checks that the call
-returns, that every conformer has a defined result, that the error word is
-set, and that the context stays usable for a normal run afterwards.
+With ``give_up_waits=True`` every wait on a row copy gives up before testing,
+as if its copy never completed.  No copy is broken: the copies in flight finish
+normally and the kernel drains them before the CTA leaves.  The test checks
+that the call returns, that every conformer has a defined result, that the
+error word is set, and that the context stays usable for a normal run
+afterwards.
 """
 import numpy as np
 import pytest
@@ -47,7 +47,7 @@ def test_a_wait_that_gives_up_ends_the_call_cleanly(precision):
     out = (torch.full((C,), -1.0, dtype=torch.float64, device="cuda"),
            torch.full((C,), -7, dtype=torch.int32, device="cuda"),
            torch.full((C,), -7, dtype=torch.int32, device="cuda"))
-    e, st, it = m.minimize_device(x, out=out, err=err, wait_spins=1, **kw)
+    e, st, it = m.minimize_device(x, out=out, err=err, give_up_waits=True, **kw)
     torch.cuda.synchronize()
     e, st, it = e.cpu().numpy(), st.cpu().numpy(), it.cpu().numpy()
     assert int(err.item()) == 1
@@ -77,7 +77,7 @@ def test_the_synchronous_call_raises_on_a_timeout():
     params, counts, pos = _streamed_batch(seed=33, n_mols=2, k=2)
     m = mm.Minimizer(params, counts)
     with pytest.raises(_lib.MMFFBError, match="bounded wait"):
-        m.minimize(pos, max_iters=50, wait_spins=1)
+        m.minimize(pos, max_iters=50, give_up_waits=True)
     r = m.minimize(pos, max_iters=50)
     assert np.isfinite(r.energies).all()
 
@@ -88,7 +88,7 @@ def test_binned_launches_report_the_error_word():
     m = mm.BinnedMinimizer(params, counts)
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     x = torch.from_numpy(pos).cuda()
-    _, st, _ = m.minimize_device(x, max_iters=50, err=err, wait_spins=1)
+    _, st, _ = m.minimize_device(x, max_iters=50, err=err, give_up_waits=True)
     torch.cuda.synchronize()
     assert int(err.item()) == 1 and bool((st == _lib.ST_TIMEOUT).all())
     x = torch.from_numpy(pos).cuda()

@@ -70,7 +70,7 @@ def _dirty_the_array():
     m = mm.Minimizer(params, counts)
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     x = torch.from_numpy(pos.astype(np.float32)).cuda()
-    _, st, _, _ = _noalloc(m, x, mm.opt_params(max_iters=20, grad_tol=1e-4, wait_spins=1,
+    _, st, _, _ = _noalloc(m, x, mm.opt_params(max_iters=20, grad_tol=1e-4, give_up_waits=True,
                                                err_word=err.data_ptr()))
     torch.cuda.synchronize()
     assert int(err.item()) == 1 and bool((st == _lib.ST_TIMEOUT).all())
