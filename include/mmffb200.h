@@ -114,10 +114,6 @@ typedef struct {
                                     before testing, as if the copy never completed, which exercises the
                                     timeout path (the kernel drains the copies in flight, its conformers
                                     end MMFFB_ST_TIMEOUT and the error word is set) */
-    int32_t two_pending;         /* inverse Hessian in global memory, register-lean mixed instance: 0 = keep
-                                    two rank-2 updates pending and store H every other iteration when the
-                                    extra shared memory leaves as many CTAs per SM (same results, half the
-                                    write-back); -1 = store after every update */
     int32_t *err_word;           /* optional device int32, zeroed by the call; 1 once the launch is done
                                     if a bounded wait gave up (the affected conformers then have status
                                     MMFFB_ST_TIMEOUT).  With or without it, mmffb_minimize's scratch

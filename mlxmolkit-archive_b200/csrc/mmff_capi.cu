@@ -112,7 +112,6 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     pl->nt = nt;
     pl->nc = nc;
     pl->msm = msm;
-    pl->two_pend = false;
     pl->smem = L.total;
     pl->rsz = rs;
     pl->gslot = mat_elems(nmax, o->history_m);
@@ -122,22 +121,6 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     };
     int fit = occupancy();
     if (fit < 0) return fit;
-    if (mixed && !lb && !msm && nc == 0 && o->two_pending >= 0) {
-        // the register-lean streamed instance: keep two updates pending and store H every
-        // other iteration, when the three extra vectors still leave as many CTAs per SM
-        Layout L2 = make_layout(nmax, nt / 32, 0, false, rs, as, mc, true);
-        pl->smem = L2.total;
-        pl->two_pend = true;
-        const int fit2 = L2.total <= (size_t)optin ? occupancy() : 0;
-        if (fit2 < 0) return fit2;
-        if (fit2 >= fit && fit2 > 0) {
-            fit = fit2;
-        } else {
-            pl->smem = L.total;
-            pl->two_pend = false;
-        }
-    }
-    if (fit < 1) return fail(MMFFB_ETOOBIG, "no CTA of this instance fits on an SM (%zu B shared)", pl->smem);
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
     int grid = sms * fit;
     if (grid > c->n_conf) grid = c->n_conf > 0 ? c->n_conf : 1;
@@ -172,7 +155,6 @@ Params make_params(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPar
     P.max_restarts = o->max_restarts < 0 ? 0 : o->max_restarts;
     P.polish64 = o->precision == MMFFB_PREC_MIXED && o->polish64 != 0;
     P.wait_spins = o->give_up_waits ? 0u : o->wait_spins ? o->wait_spins : kMaxWaitSpins;
-    P.two_pending = pl.two_pend ? 1 : 0;
     P.ls_evals = ls_evals;
     P.nmax = c->max_atoms;
     P.pos = pos;

@@ -52,15 +52,22 @@ struct MolV {
     int boff, bnch, aoff, anch, soff, snch, ooff, onch, toff, tnch;
 };
 
+// Data read once per conformer (descriptor, slot, coordinates, per-atom staging) is
+// loaded through L2 (ld.global.cg): a serving worker reads slots that the host
+// publishes while it runs, and L1 lines loaded for an earlier slot may hold the
+// same lines' old contents.  The bonded records, read every evaluation, keep the
+// read-only cache: each molecule's records start on a 512-byte boundary, so no
+// line holds two molecules' records.
 __device__ __forceinline__ MolV load_mol(const int32_t *desc, int m) {
     const int32_t *d = desc + (size_t)m * MMFFB_MOL_DESC_INTS;
     MolV v;
-    v.n = d[MMFFB_MD_N]; v.atom_off = d[MMFFB_MD_ATOM_OFF]; v.ncls = d[MMFFB_MD_NCLS];
-    v.cls_off = d[MMFFB_MD_CLS_OFF]; v.mask_off = d[MMFFB_MD_MASK_OFF]; v.diel = d[MMFFB_MD_DIEL];
-    v.boff = d[MMFFB_MD_B_OFF]; v.bnch = d[MMFFB_MD_B_NCH]; v.aoff = d[MMFFB_MD_A_OFF];
-    v.anch = d[MMFFB_MD_A_NCH]; v.soff = d[MMFFB_MD_S_OFF]; v.snch = d[MMFFB_MD_S_NCH];
-    v.ooff = d[MMFFB_MD_O_OFF]; v.onch = d[MMFFB_MD_O_NCH]; v.toff = d[MMFFB_MD_T_OFF];
-    v.tnch = d[MMFFB_MD_T_NCH];
+    v.n = __ldcg(d + MMFFB_MD_N); v.atom_off = __ldcg(d + MMFFB_MD_ATOM_OFF); v.ncls = __ldcg(d + MMFFB_MD_NCLS);
+    v.cls_off = __ldcg(d + MMFFB_MD_CLS_OFF); v.mask_off = __ldcg(d + MMFFB_MD_MASK_OFF);
+    v.diel = __ldcg(d + MMFFB_MD_DIEL);
+    v.boff = __ldcg(d + MMFFB_MD_B_OFF); v.bnch = __ldcg(d + MMFFB_MD_B_NCH); v.aoff = __ldcg(d + MMFFB_MD_A_OFF);
+    v.anch = __ldcg(d + MMFFB_MD_A_NCH); v.soff = __ldcg(d + MMFFB_MD_S_OFF); v.snch = __ldcg(d + MMFFB_MD_S_NCH);
+    v.ooff = __ldcg(d + MMFFB_MD_O_OFF); v.onch = __ldcg(d + MMFFB_MD_O_NCH); v.toff = __ldcg(d + MMFFB_MD_T_OFF);
+    v.tnch = __ldcg(d + MMFFB_MD_T_NCH);
     return v;
 }
 
@@ -83,7 +90,6 @@ struct Params {
     int max_restarts;
     int polish64;      // mixed precision: FP64 line-search energies once the FP32 ones stall
     uint32_t wait_spins;   // tests of a ring stage's completion before its wait gives up (0: none)
-    int two_pending;   // streamed FP32 H: store it every other iteration, two updates pending
     int32_t *ls_evals;
     int *err;          // set when a bounded wait gave up (never expected): the caller's word or scratch_err
     int *scratch_err;  // the scratch head's error word (byte 4), set as well
@@ -133,15 +139,15 @@ __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) & ~(
 constexpr int kStages = 4;         // rows of H in flight per warp (TMA ring)
 
 struct Layout {
-    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, pxi2, pc2, pr2, gbuf, cls, q, qf, mask, tab, red,
-        rho, alpha, ring, mbar, mat, total;
+    size_t pos4, pos4d, x, g, dir, xo, dg, hp, hq, pxi, pc, pr, gbuf, cls, q, qf, mask, tab, red, rho, alpha,
+        ring, mbar, mat, total;
 };
 
 // row stride of a dense inverse Hessian in global memory: 16-byte multiple for TMA rows
 __host__ __device__ __forceinline__ int hld(int n) { return (n + 3) & ~3; }
 
 __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, bool mat_in_smem,
-                                              size_t rs, size_t as, int max_classes = 32, bool two_pend = false) {
+                                              size_t rs, size_t as, int max_classes = 32) {
     Layout L;
     size_t nv = (size_t)((3 * nmax + 3) & ~3);
     size_t o = 0;
@@ -157,9 +163,6 @@ __host__ __device__ inline Layout make_layout(int nmax, int nwarps, int hist_m, 
     L.pxi = o; o = al16(o + nv * rs);
     L.pc = o; o = al16(o + nv * rs);
     L.pr = o; o = al16(o + nv * rs);
-    L.pxi2 = o; o = al16(o + (two_pend ? nv * rs : 0));   // the second pending update
-    L.pc2 = o; o = al16(o + (two_pend ? nv * rs : 0));
-    L.pr2 = o; o = al16(o + (two_pend ? nv * rs : 0));
     L.gbuf = o; o = al16(o + (size_t)nwarps * nv * rs);
     L.cls = o; o = al16(o + (size_t)nmax * 4);
     L.q = o; o = al16(o + (size_t)nmax * 8);
@@ -345,16 +348,16 @@ __device__ __forceinline__ void stage_molecule(const Params &P, const MolV &m, i
                                                uint32_t *mask, float2 *tab) {
     const int N = m.n, W = (N + 31) >> 5;
     for (int a = threadIdx.x; a < N; a += NT) {
-        cls[a] = P.b.atom_cls[m.atom_off + a];
-        const double q = P.b.atom_q[m.atom_off + a];
+        cls[a] = __ldcg(P.b.atom_cls + m.atom_off + a);
+        const double q = __ldcg(P.b.atom_q + m.atom_off + a);
         qa[a] = q;
         qf[a] = (float)q;
     }
     const uint32_t *gm = P.b.pair_mask + m.mask_off;
-    for (int k = threadIdx.x; k < 2 * N * W; k += NT) mask[k] = gm[k];
+    for (int k = threadIdx.x; k < 2 * N * W; k += NT) mask[k] = __ldcg(gm + k);
     const float2 *gt = reinterpret_cast<const float2 *>(P.b.cls_tab) + m.cls_off;
     for (int k = threadIdx.x; k < m.ncls * m.ncls; k += NT) {
-        float2 v = gt[k];
+        float2 v = __ldcg(gt + k);
         if (IR) v.x = Num<float>::rcp(v.x > 1e-8f ? v.x : 1e-8f);
         tab[k] = v;
     }
@@ -544,10 +547,8 @@ __device__ __forceinline__ A eval_terms(const Params &P, const MolV &m, const R 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>
 struct Opt {
     static constexpr int NW = NT / 32;
-    // the register-lean streamed FP32 instance may keep two updates pending (P.two_pending)
-    static constexpr bool kTwoPend = !MSM && NC == 0 && sizeof(R) == 4 && !LB;
     const Params &P;
-    R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *pxi2, *pc2, *pr2, *gbuf, *mat;
+    R *pos4, *x, *g, *dir, *xo, *dg, *hp, *hq, *pxi, *pc, *pr, *gbuf, *mat;
     double *pos4d;     // FP64 copy of pos4 (float R only)
     R *ring;           // TMA row ring (streamed H pass)
     uint64_t *mbar;    // one mbarrier per ring stage and warp
@@ -567,8 +568,7 @@ struct Opt {
     int N, n, nv;
 
     __device__ Opt(const Params &p, unsigned char *sm, int *abort_ = nullptr) : P(p), abort_flag(abort_), rsel(0) {
-        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes,
-                               p.two_pending != 0);
+        Layout L = make_layout(p.nmax, NW, LB ? p.hist_m : 0, MSM, sizeof(R), sizeof(A), p.b.max_classes);
         pos4 = (R *)(sm + L.pos4); x = (R *)(sm + L.x); g = (R *)(sm + L.g); dir = (R *)(sm + L.dir);
         pos4d = (double *)(sm + L.pos4d);
         use64 = false;
@@ -578,7 +578,6 @@ struct Opt {
         ldh = 0;
         xo = (R *)(sm + L.xo); dg = (R *)(sm + L.dg); hp = (R *)(sm + L.hp); hq = (R *)(sm + L.hq);
         pxi = (R *)(sm + L.pxi); pc = (R *)(sm + L.pc); pr = (R *)(sm + L.pr); gbuf = (R *)(sm + L.gbuf);
-        pxi2 = (R *)(sm + L.pxi2); pc2 = (R *)(sm + L.pc2); pr2 = (R *)(sm + L.pr2);
         cls = (int *)(sm + L.cls); qa = (double *)(sm + L.q); red = (A *)(sm + L.red);
         qf = (float *)(sm + L.qf); mask = (uint32_t *)(sm + L.mask); tab = (float2 *)(sm + L.tab);
         ms.cls = cls; ms.qa = qa; ms.qf = qf; ms.mask = mask; ms.tab = tab;
@@ -816,13 +815,7 @@ struct Opt {
     // rows of H and the vectors are padded to a multiple of 4 with zeros) and two
     // rows per step, so each vector load from shared memory serves two rows and a
     // warp keeps two row copies of its TMA ring in use at once.
-    //
-    // npend rank-2 updates are pending (0, 1 or 2; the older in pxi/pc/pr, the newer
-    // in pxi2/pc2/pr2) and applied to each element in that order, so the values equal
-    // those of storing after every update; the rows are stored only when `store`.
-    // With two pending updates stored every other iteration, H is written back half
-    // as often for the same results.
-    __device__ __forceinline__ void hpass_stream_v4(int npend, bool store) {
+    __device__ __forceinline__ void hpass_stream_v4(bool pending) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int ldr = hld(3 * P.nmax);
         float *rw = (float *)ring + (size_t)warp * kStages * ldr;
@@ -831,7 +824,6 @@ struct Opt {
         const uint32_t bytes = (uint32_t)(ldh * sizeof(float));
         const int n4 = ldh >> 2;
         const float4 *X4 = (const float4 *)pxi, *C4 = (const float4 *)pc;
-        const float4 *Y4 = (const float4 *)pxi2, *D24 = (const float4 *)pc2;
         const float4 *G4 = (const float4 *)g, *D4 = (const float4 *)dg;
         float *H = (float *)mat;
         if (lane == 0) {
@@ -866,52 +858,34 @@ struct Opt {
                 const int i0 = warp + NW * t, i1 = i0 + NW;
                 const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
                 float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
-                const bool p1 = npend >= 1, p2 = npend >= 2;
-                const float r0 = p1 ? (float)pr[i0] : 0.f, x0 = p1 ? (float)pxi[i0] : 0.f;
-                const float r1 = (p1 && two) ? (float)pr[i1] : 0.f, x1 = (p1 && two) ? (float)pxi[i1] : 0.f;
-                const float q0 = p2 ? (float)pr2[i0] : 0.f, y0 = p2 ? (float)pxi2[i0] : 0.f;
-                const float q1 = (p2 && two) ? (float)pr2[i1] : 0.f, y1 = (p2 && two) ? (float)pxi2[i1] : 0.f;
-                float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+                const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
+                const float r1 = (pending && two) ? (float)pr[i1] : 0.f, x1 = (pending && two) ? (float)pxi[i1] : 0.f;
+                float a0 = 0.f, q0 = 0.f, a1 = 0.f, q1 = 0.f;
                 for (int c = lane; c < n4; c += 32) {
                     float4 h0 = A0[c];
                     float4 h1 = two ? A1[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (p1) {
+                    if (pending) {
                         const float4 px = X4[c], pv = C4[c];
                         h0.x = fmaf(x0, pv.x, fmaf(px.x, r0, h0.x));
                         h0.y = fmaf(x0, pv.y, fmaf(px.y, r0, h0.y));
                         h0.z = fmaf(x0, pv.z, fmaf(px.z, r0, h0.z));
                         h0.w = fmaf(x0, pv.w, fmaf(px.w, r0, h0.w));
+                        W0[c] = h0;
                         if (two) {
                             h1.x = fmaf(x1, pv.x, fmaf(px.x, r1, h1.x));
                             h1.y = fmaf(x1, pv.y, fmaf(px.y, r1, h1.y));
                             h1.z = fmaf(x1, pv.z, fmaf(px.z, r1, h1.z));
                             h1.w = fmaf(x1, pv.w, fmaf(px.w, r1, h1.w));
+                            W1[c] = h1;
                         }
-                    }
-                    if (p2) {
-                        const float4 py = Y4[c], pw = D24[c];
-                        h0.x = fmaf(y0, pw.x, fmaf(py.x, q0, h0.x));
-                        h0.y = fmaf(y0, pw.y, fmaf(py.y, q0, h0.y));
-                        h0.z = fmaf(y0, pw.z, fmaf(py.z, q0, h0.z));
-                        h0.w = fmaf(y0, pw.w, fmaf(py.w, q0, h0.w));
-                        if (two) {
-                            h1.x = fmaf(y1, pw.x, fmaf(py.x, q1, h1.x));
-                            h1.y = fmaf(y1, pw.y, fmaf(py.y, q1, h1.y));
-                            h1.z = fmaf(y1, pw.z, fmaf(py.z, q1, h1.z));
-                            h1.w = fmaf(y1, pw.w, fmaf(py.w, q1, h1.w));
-                        }
-                    }
-                    if (store) {
-                        W0[c] = h0;
-                        if (two) W1[c] = h1;
                     }
                     const float4 gg = G4[c], dd = D4[c];
                     a0 = fmaf(h0.w, gg.w, fmaf(h0.z, gg.z, fmaf(h0.y, gg.y, fmaf(h0.x, gg.x, a0))));
-                    b0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, b0))));
+                    q0 = fmaf(h0.w, dd.w, fmaf(h0.z, dd.z, fmaf(h0.y, dd.y, fmaf(h0.x, dd.x, q0))));
                     a1 = fmaf(h1.w, gg.w, fmaf(h1.z, gg.z, fmaf(h1.y, gg.y, fmaf(h1.x, gg.x, a1))));
-                    b1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, b1))));
+                    q1 = fmaf(h1.w, dd.w, fmaf(h1.z, dd.z, fmaf(h1.y, dd.y, fmaf(h1.x, dd.x, q1))));
                 }
-                v[4 * u] = a0; v[4 * u + 1] = b0; v[4 * u + 2] = a1; v[4 * u + 3] = b1;
+                v[4 * u] = a0; v[4 * u + 1] = q0; v[4 * u + 2] = a1; v[4 * u + 3] = q1;
                 __syncwarp();   // every lane's reads of both stages before they are refilled
                 if (lane == 0) {
                     fence_proxy_async_smem();
@@ -928,7 +902,7 @@ struct Opt {
                 }
             }
             if (aborted) break;
-            // lanes l and l^1 now hold the sum of value l >> 1: pair u = value / 4, then a0 b0 a1 b1
+            // lanes l and l^1 now hold the sum of value l >> 1: pair u = value / 4, then a0 q0 a1 q1
             const float sum = reduce16(v);
             const int val = lane >> 1, tr = t0 + 2 * (val >> 2) + ((val >> 1) & 1);
             if (!(lane & 1) && tr < nrows) {
@@ -996,24 +970,22 @@ struct Opt {
     __device__ void run(int conf) {
         const int tid = threadIdx.x;
         const KConst &K = P.K;
-        m = load_mol(P.b.mol_desc, P.c.conf_mol[conf]);
+        m = load_mol(P.b.mol_desc, __ldcg(P.c.conf_mol + conf));
         N = m.n;
         n = 3 * N;
         nv = (3 * P.nmax + 3) & ~3;
         use64 = false;
-        const float *gp = P.pos + P.c.conf_coord[conf];
+        const int64_t coord = __ldcg(reinterpret_cast<const long long *>(P.c.conf_coord) + conf);
+        const float *gp = P.pos + coord;
         for (int k = tid; k < n; k += NT) {
-            R v = (R)gp[k];
+            R v = (R)__ldcg(gp + k);
             x[k] = v;
             setpos(k, v);
         }
         stage_molecule<NT, sizeof(R) == 4>(P, m, cls, qa, qf, mask, tab);
         ldh = MSM ? n : hld(n);
         // zero vector pads: the float4 pass reads columns up to hld(n)
-        for (int k = n + tid; k < nv; k += NT) {
-            g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0);
-            if (kTwoPend && P.two_pending) { pxi2[k] = R(0); pc2[k] = R(0); }
-        }
+        for (int k = n + tid; k < nv; k += NT) { g[k] = R(0); dg[k] = R(0); pxi[k] = R(0); pc[k] = R(0); }
         if (!LB) reset_matrix();
         __syncthreads();
 
@@ -1043,8 +1015,7 @@ struct Opt {
         int status = MMFFB_ST_MAXIT;
         int it = 0, done_iters = 0, nevals = 0, restarts = 0;
         bool fresh = true;     // direction is -g (start or just after a restart)
-        int npend = 0;         // rank-2 updates not yet stored in H (at most 2, else 1)
-        const bool two_pend = kTwoPend && P.two_pending;
+        bool pending = false;  // a rank-2 update not yet applied to H
         int hcount = 0, hidx = 0;
         if (!isfinite((double)E) || !isfinite((double)gs_[0])) {
             status = MMFFB_ST_NONFINITE;
@@ -1083,7 +1054,7 @@ struct Opt {
                         // uphill quasi-Newton direction: restart from steepest descent
                         ++restarts;
                         fresh = true;
-                        npend = 0;
+                        pending = false;
                         hcount = 0;
                         hidx = 0;
                         reset_matrix();
@@ -1151,7 +1122,7 @@ struct Opt {
                         // no decrease along the quasi-Newton direction: restart from -g
                         ++restarts;
                         fresh = true;
-                        npend = 0;
+                        pending = false;
                         hcount = 0;
                         hidx = 0;
                         reset_matrix();
@@ -1221,11 +1192,9 @@ struct Opt {
                 }
                 if (!LB) {
                     __syncthreads();
-                    const bool store = two_pend ? npend == 2 : npend > 0;
-                    if constexpr (kTwoPend) hpass_stream_v4(npend, store);
-                    else if (MSM) hpass(npend > 0);
-                    else hpass_stream(npend > 0);
-                    if (store) npend = 0;
+                    if constexpr (!MSM && NC == 0 && sizeof(R) == 4) hpass_stream_v4(pending);
+                    else if (MSM) hpass(pending);
+                    else hpass_stream(pending);
                     __syncthreads();
                     if (!MSM && *(volatile int *)abort_flag) { status = MMFFB_ST_TIMEOUT; break; }
                     A d6[6] = {A(0), A(0), A(0), A(0), A(0), A(0)}, z[1] = {A(0)};
@@ -1245,18 +1214,17 @@ struct Opt {
                         const A al = fi * (A(1) + fae * fi);
                         const R cxg = (R)(al * d6[4]), cqg = (R)(fi * d6[5]), fxg = (R)(fi * d6[4]);
                         const R rfi = (R)fi, ral = (R)al;
-                        // the update joins the pending ones (the first or the second slot)
-                        R *ux = npend == 0 ? pxi : pxi2, *uc = npend == 0 ? pc : pc2, *ur = npend == 0 ? pr : pr2;
                         for (int k = tid; k < n; k += NT) {
                             const R xk = xo[k], qk = hq[k];
                             dir[k] = -(hp[k] + cxg * xk - cqg * xk - fxg * qk);
-                            ux[k] = xk;
-                            uc[k] = -rfi * qk;
-                            ur[k] = ral * xk - rfi * qk;
+                            pxi[k] = xk;
+                            pc[k] = -rfi * qk;
+                            pr[k] = ral * xk - rfi * qk;
                         }
-                        ++npend;
+                        pending = true;
                     } else {
                         for (int k = tid; k < n; k += NT) dir[k] = -hp[k];
+                        pending = false;
                     }
                 } else {
                     // L-BFGS history update (lbfgs_tg.metal:247-262)
@@ -1280,7 +1248,7 @@ struct Opt {
         if (status != MMFFB_ST_NONFINITE || it < P.max_iters)
             done_iters = it < P.max_iters ? it + (status == MMFFB_ST_SLOPE ? 0 : 1) : P.max_iters;
         __syncthreads();
-        float *op = P.pos + P.c.conf_coord[conf];
+        float *op = P.pos + coord;
         for (int k = tid; k < n; k += NT) op[k] = (float)x[k];
         if (tid == 0) {
             P.energy[conf] = (double)E;
@@ -1414,7 +1382,6 @@ __global__ void __launch_bounds__(NT) check64_kernel(const Params P, const doubl
 struct Plan {
     int nt, nc;
     bool msm;
-    bool two_pend;     // streamed FP32 H with two pending updates (stored every other iteration)
     size_t smem;
     int grid;
     size_t gslot;      // matrix elements per CTA slot when not in shared memory

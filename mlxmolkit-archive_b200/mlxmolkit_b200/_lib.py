@@ -40,8 +40,7 @@ class MMFFOptParams(ctypes.Structure):
                 ("exit_test", ctypes.c_int32), ("check_every", ctypes.c_int32),
                 ("atom_grad_scale", ctypes.c_float), ("max_restarts", ctypes.c_int32),
                 ("polish64", ctypes.c_int32), ("hpass_lean", ctypes.c_int32),
-                ("wait_spins", ctypes.c_uint32), ("give_up_waits", ctypes.c_int32),
-                ("two_pending", ctypes.c_int32), ("err_word", P)]
+                ("wait_spins", ctypes.c_uint32), ("give_up_waits", ctypes.c_int32), ("err_word", P)]
 
 
 # (MMFFTermsHost field, MMFFParams field, ctypes element type) in the header's order

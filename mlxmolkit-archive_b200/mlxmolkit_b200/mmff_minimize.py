@@ -113,18 +113,15 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
                polish64: Optional[bool] = None, hpass_lean: bool = True, wait_spins: int = 0,
-               err_word: int = 0, two_pending: bool = True, give_up_waits: bool = False) -> _lib.MMFFOptParams:
+               err_word: int = 0, give_up_waits: bool = False) -> _lib.MMFFOptParams:
     """Launch options; ``polish64`` (default: on for mixed precision) switches a conformer's
     line-search energies to FP64 once the FP32 ones stall.  ``err_word``: device address of an
     int32 that the launch sets to 1 when a bounded wait gives up; ``wait_spins`` bounds those
     waits (0: the library default); ``give_up_waits`` makes every such wait give up at once (a test
-    switch that exercises the timeout path).  ``two_pending``: the
-    streamed FP32 inverse Hessian is stored every other iteration where that keeps the occupancy
-    (same results)."""
+    switch that exercises the timeout path)."""
     o = _lib.MMFFOptParams()
     o.wait_spins = int(wait_spins)
     o.give_up_waits = int(bool(give_up_waits))
-    o.two_pending = 0 if two_pending else -1
     o.err_word = int(err_word) or None
     o.max_restarts = int(max_restarts)
     o.polish64 = int(precision == "mixed" if polish64 is None else bool(polish64))
@@ -204,7 +201,7 @@ class Minimizer:
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
                         hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
-                        wait_spins: int = 0, two_pending: bool = True, give_up_waits: bool = False):
+                        wait_spins: int = 0, give_up_waits: bool = False):
         """Minimise in place on the device; returns (energy, status, iters) device tensors.
 
         ``evals`` (optional int32 device tensor, one per conformer) receives the
@@ -223,7 +220,7 @@ class Minimizer:
             e, st, it = out
         o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode, threads, ctas_per_sm,
                        exit_test, check_every, atom_grad_scale, max_restarts, polish64, hpass_lean,
-                       wait_spins, err.data_ptr() if err is not None else 0, two_pending, give_up_waits)
+                       wait_spins, err.data_ptr() if err is not None else 0, give_up_waits)
         bd, cd = self.batch.desc(), self.confs.desc()
         nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
         if nbytes == 0 and C > 0:
@@ -376,17 +373,21 @@ class BinnedMinimizer(Minimizer):
                                   "stream": torch.cuda.Stream(device=self.batch.device), "scratch": None,
                                   "cost": float(np.sum((3.0 * nconf[sel]) ** 2))})
             lo = hi
-        # largest molecules first: their conformers take longest, and a class launched
-        # earlier takes the SMs first (longest-processing-time order across classes)
+        # largest molecules first: their conformers take longest, so their class gets the SMs
+        # first (longest-processing-time order across classes).  Launch order alone does not
+        # ensure it -- the launches of the classes are queued on their streams within
+        # microseconds -- so each class's stream also gets a priority, the largest molecules'
+        # the highest: the block scheduler then places that class's CTAs before any other's.
         self.bins.sort(key=lambda b: -b["hi"])
+        for rank, b in enumerate(self.bins):
+            b["stream"] = torch.cuda.Stream(device=self.batch.device, priority=-(len(self.bins) - 1 - rank))
 
     def minimize_device(self, pos_dev, *, max_iters: int, grad_tol: float = 1e-4, history_m: int = 0,
                         precision: str = "mixed", consts=TG_CONSTS, mode=MODE_TG, threads: int = 0,
                         ctas_per_sm: int = 0, exit_test: int = _lib.EXIT_TG, check_every: int = 0,
                         atom_grad_scale: float = 1.0, max_restarts: int = 0, polish64=None,
                         hpass_lean: bool = True, stream=None, out=None, evals=None, err=None,
-                        wait_spins: int = 0, two_pending: bool = True, give_up_waits: bool = False,
-                        time_bins=False):
+                        wait_spins: int = 0, give_up_waits: bool = False, time_bins=False):
         """As ``Minimizer.minimize_device``, one launch per size class.  With
         ``time_bins`` each launch is bracketed by timing events on its own stream;
         ``bin_times_ms()`` reads them after a synchronize."""
@@ -409,7 +410,7 @@ class BinnedMinimizer(Minimizer):
             o = opt_params(max_iters, grad_tol, history_m, precision, consts, mode,
                            threads or cfg.get("threads", 0), ctas_per_sm or cfg.get("ctas_per_sm", 0),
                            exit_test, check_every, atom_grad_scale, max_restarts, polish64,
-                           bool(cfg.get("lean", hpass_lean)), wait_spins, 0, two_pending, give_up_waits)
+                           bool(cfg.get("lean", hpass_lean)), wait_spins, 0, give_up_waits)
             cd = b["confs"].desc()
             nbytes = L.mmffb_minimize_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(o))
             if b["scratch"] is None or b["scratch"].numel() < nbytes:

@@ -1,13 +1,16 @@
 """Small profiling case of the optimizer kernels, sized for an ncu capture.
 
 One size-binned minimisation of ``--mols`` seeded drug-like molecules x ``--k``
-conformers (heavy atoms 8-70, at most 150 atoms), mixed precision, dense
-BFGS, at most 1000 iterations.  At the defaults (60 x 10) the global-slot
-size class holds about 300 conformers of 75-150 atoms, whose inverse-Hessian
-slots (one per CTA, 296 CTAs) take more than the 126 MB L2, so DRAM counters
-keep their meaning, while the device holds well under 1 GB.
+conformers (heavy atoms ``--lo``-``--hi``, default 8-70, at most 150 atoms),
+mixed precision, dense BFGS, at most 1000 iterations.  At the defaults
+(60 x 10) the global-slot size class holds about 300 conformers of 75-150
+atoms, whose inverse-Hessian slots (one per CTA, 296 CTAs) take more than the
+126 MB L2, so DRAM counters keep their meaning, while the device holds well
+under 1 GB.  Small heavy-atom ranges fill the GPU with one shared-memory size
+class instead: ``--lo 4 --hi 8`` (up to 24 atoms), ``--lo 10 --hi 16``
+(25-48 atoms), each with enough conformers for every SM.
 
-Usage: python -m mlxmolkit_b200.profile_case [--mols 60] [--k 10] [--repeat 1]
+Usage: python -m mlxmolkit_b200.profile_case [--mols 60] [--k 10] [--lo 8] [--hi 70] [--repeat 1]
 """
 from __future__ import annotations
 
@@ -27,9 +30,11 @@ def main():
     ap.add_argument("--k", type=int, default=10)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--lo", type=int, default=8, help="fewest heavy atoms")
+    ap.add_argument("--hi", type=int, default=70, help="most heavy atoms")
     a = ap.parse_args()
     import torch
-    mols = synth.make_molecules(a.mols, a.k, a.seed, 8, 70, max_atoms=150)
+    mols = synth.make_molecules(a.mols, a.k, a.seed, a.lo, a.hi, max_atoms=150)
     params = [extract_mmff_params(m) for m in mols]
     pos = np.concatenate([np.stack([c.pos for c in m.GetConformers()]).reshape(-1)
                           for m in mols]).astype(np.float32)

@@ -63,7 +63,8 @@ import numpy as np
 from . import _lib
 from . import mmff_minimize as mm
 from .mmff_params import extract_mmff_params
-from .pack import MD_NCLS, conformer_index, lpt_order, merge_packed, pack_molecules
+from .pack import (MD_ATOM_OFF, MD_B_OFF, MD_CLS_OFF, MD_MASK_OFF, MD_NCLS, merge_packed,
+                   pack_molecules)
 
 
 @dataclass
@@ -229,6 +230,7 @@ class _Half:
         self.done_np = self.done_buf.array
         self.done_dev = self.done_buf.device_ptr
         self.workers: list = []                   # (end event, scratch index, launch time) of its launches
+        self.pending: list = []                   # queue writes waiting for their data: (event, tail | None)
         self.closed = True
         self.requests: list = []
         self.n_mol = self.n_row = self.n_atom = self.n_pair = self.n_word = self.n_slot = self.n_coord = 0
@@ -272,7 +274,7 @@ class _Half:
 
     def idle(self) -> bool:
         """Closed, no worker running and every request completed: free for a new generation."""
-        return self.closed and not self.worker_running() and not self.requests
+        return self.closed and not self.pending and not self.worker_running() and not self.requests
 
 
 class _ClassState:
@@ -396,7 +398,7 @@ class MMFFServer:
         if hit is None:
             params = extract_mmff_params(r.mol, conf_id=r.mol.GetConformers()[0].GetId()
                                          if r.mol.GetNumConformers() else 0, mmff_variant=r.variant)
-            packed = pack_molecules([params])
+            packed = _chunk_aligned(pack_molecules([params]))
             hit = (params, packed, size_class(int(params.n_atoms), int(packed.mol_desc[0, MD_NCLS])))
             if key is not None:
                 with self.lock:
@@ -448,16 +450,37 @@ class MMFFServer:
         return other
 
     def _close_half(self, cs: _ClassState, h: _Half) -> None:
-        """No more slots: the worker ends once it has claimed every published one."""
-        torch = self.torch
-        with torch.cuda.stream(cs.copy_stream):
-            h.ctl[2:3].copy_(torch.ones(1, dtype=torch.int32).pin_memory(), non_blocking=True)
+        """No more slots: the worker ends once it has claimed every published one.  The close flag
+        is written after the half's pending tails (in order)."""
+        h.pending.append((None, None))
         h.closed = True
+
+    def _flush(self, cs: _ClassState) -> None:
+        """Write the queue words whose data has landed, in order: a tail only once the host has
+        seen the copies of its slots' data complete, so that a running worker never claims a slot
+        before its tables and coordinates are in device memory; the close flag after the tails."""
+        torch = self.torch
+        for h in cs.halves:
+            wrote = False
+            while h.pending:
+                ev, tail = h.pending[0]
+                if ev is not None and not ev.query():
+                    break
+                h.pending.pop(0)
+                with torch.cuda.stream(cs.copy_stream):
+                    if tail is None:
+                        h.ctl[2:3].copy_(torch.ones(1, dtype=torch.int32).pin_memory(), non_blocking=True)
+                    else:
+                        h.ctl[1:2].copy_(torch.tensor([tail], dtype=torch.int32).pin_memory(), non_blocking=True)
+                        wrote = True
+            if wrote:
+                ready = torch.cuda.Event()
+                ready.record(cs.copy_stream)
+                self._ensure_worker(cs, h, ready)
 
     def _publish(self, cs: _ClassState, h: _Half, reqs) -> None:
         """Copy the requests' tables, slot descriptors and coordinates into their reserved, contiguous
-        places in the half, then the new tail (ordered after them on the copy stream), and start a
-        worker if none is running."""
+        places in the half; the new tail follows once they have landed (``_flush``)."""
         torch = self.torch
         pk = merge_packed([r.packed for r in reqs])
         m0, row0, atom0, pair0, word0, slot0, coord0 = reqs[0].base
@@ -490,10 +513,9 @@ class MMFFServer:
             put(h.conf_mol, slot0, conf_mol, np.int32)
             put(h.conf_coord, slot0, coord, np.int64)
             put(h.pos, coord0, pos, np.float32)
-            put(h.ctl, 1, np.array([slot0 + len(conf_mol)], np.int32), np.int32)     # the new tail
-            ready = torch.cuda.Event()
-            ready.record(cs.copy_stream)
-        self._ensure_worker(cs, h, ready)
+            landed = torch.cuda.Event()
+            landed.record(cs.copy_stream)
+        h.pending.append((landed, slot0 + len(conf_mol)))     # the new tail, once the data has landed
 
     def _ensure_worker(self, cs: _ClassState, h: _Half, ready) -> None:
         """Start a worker on h unless a recent one runs: a worker older than its idle limit may
@@ -551,7 +573,7 @@ class MMFFServer:
                 self.copying.append((r, ev, hp, he, hs))
             h.requests = keep
             # a worker that ended on an empty queue leaves later slots unclaimed: start another
-            if keep and not h.worker_running():
+            if keep and not h.pending and not h.worker_running():
                 ready = torch.cuda.Event()
                 ready.record(cs.copy_stream)
                 self._ensure_worker(cs, h, ready)
@@ -606,6 +628,19 @@ class MMFFServer:
             self._close_half(cs, h)
         self.waiting = keep
 
+    def _fail_all(self, exc: BaseException) -> None:
+        """Complete every request not yet completed with ``exc``: waiting, published, copying."""
+        open_reqs = list(self.waiting) + [item[0] for item in self.copying]
+        for cs in self.classes.values():
+            for h in cs.halves:
+                open_reqs += h.requests
+                h.requests = []
+        for r in open_reqs:
+            if not r.future.done():
+                r.future.set_exception(exc)
+        self.waiting = []
+        self.copying = []
+
     def _loop(self) -> None:
         torch = self.torch
         torch.cuda.set_device(self.device)
@@ -617,22 +652,24 @@ class MMFFServer:
                 pass
             try:
                 for cs in list(self.classes.values()):
+                    self._flush(cs)
                     self._collect(cs)
                 self._finish_copies()
                 self._admit()
-            except BaseException as exc:    # pragma: no cover - fail every open request
+            except BaseException as exc:    # pragma: no cover - fail every open request with it
+                import sys
+                import traceback
+                traceback.print_exc(file=sys.stderr)
                 self.error = exc
-                for r in self.waiting:
-                    if not r.future.done():
-                        r.future.set_exception(exc)
-                self.waiting = []
-            pending = any(h.requests for cs in self.classes.values() for h in cs.halves)
+                self._fail_all(exc)
+            pending = any(h.requests or h.pending for cs in self.classes.values() for h in cs.halves)
             if self.stop_flag.is_set() and not self.waiting and not pending and not self.copying \
                     and self.incoming.empty():
                 for cs in self.classes.values():
                     for h in cs.halves:
                         if not h.closed:
                             self._close_half(cs, h)
+                    self._flush(cs)
                 for cs in self.classes.values():
                     cs.copy_stream.synchronize()
                     for st in cs.compute_streams:
@@ -645,6 +682,19 @@ class _EmptyHalf:
     """Counters of an empty half (the capacity check of a request alone)."""
 
     n_mol = n_row = n_atom = n_pair = n_word = n_slot = n_coord = 0
+
+
+def _chunk_aligned(pk):
+    """The molecule's bonded records padded to whole chunks of 32 (512 bytes): a molecule without
+    bonded terms packs as one invalid record, and every molecule's records must start on a
+    512-byte boundary of the arena (a worker keeps them in its read-only cache)."""
+    rows = len(pk.bonded)
+    if rows % 32 == 0:
+        return pk
+    pad = np.zeros((32 - rows % 32, 4), dtype=np.uint32)
+    pad[:, 0] = 0xFFFFFFFF
+    pk.bonded = np.concatenate([pk.bonded, pad])
+    return pk
 
 
 def _fits(h, c: _Caps, pk, k: int, n_atoms: int) -> bool:

@@ -87,21 +87,3 @@ def test_dense_lean_instance_reaches_the_fp64_minimum(golden_large):
     assert np.all(np.abs(r.energies - eo) <= 0.1), r.energies - eo
     assert np.all(r.grad_rms_fp64 < 0.05), r.grad_rms_fp64
 
-
-def test_two_pending_updates_give_the_same_results(golden_large):
-    """The register-lean streamed instance stores the inverse Hessian every other iteration with
-    two rank-2 updates pending; each element gets the same operations in the same order, so the
-    results equal those of storing after every update bit for bit."""
-    import torch
-    params, counts, pos = _batch(golden_large, DENSE)
-    m = mm.Minimizer(params, counts)
-    out = []
-    for two in (True, False):
-        x = torch.from_numpy(pos).cuda()
-        ev = torch.zeros(m.confs.n_conf, dtype=torch.int32, device="cuda")
-        e, st, it = m.minimize_device(x, max_iters=400, evals=ev, two_pending=two)
-        torch.cuda.synchronize()
-        out.append([t.cpu().numpy() for t in (x, e, st, it, ev)])
-    for a, b, name in zip(out[0], out[1], ("positions", "energy", "status", "iters", "ls_evals")):
-        assert np.array_equal(a, b), name
-    assert out[0][3].min() > 10
