@@ -347,6 +347,10 @@ typedef struct {
 int mmffb_host_alloc_mapped(size_t bytes, void **host, void **device);
 int mmffb_host_free(void *host);
 
+/* CTAs of the persistent grid mmffb_minimize would launch for these conformers and options
+ * (as many as fit on the device, at most one per conformer), or a negative MMFFB_E* code. */
+int32_t mmffb_minimize_ctas(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt);
+
 /* Bytes of device scratch mmffb_minimize_queue needs (max_ctas: 0 = as many CTAs as fit). */
 size_t mmffb_queue_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,
                                  int32_t max_ctas);

@@ -96,7 +96,7 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
             if (nt == 512) nt = 256;
             if (nt == 64 && n > 128) nt = 128;
             nc = nt == 64 ? 4 : 8;
-            if (n > 32 * nc) msm = false;
+            if (nc > 0 && n > 32 * nc) msm = false;   // register-cached columns cover 32 * nc
         }
         if (!msm) {
             // streamed H: register-cached columns (1 CTA/SM), or the register-lean form
@@ -300,6 +300,15 @@ int mmffb_host_alloc_mapped(size_t bytes, void **host, void **device) {
 int mmffb_host_free(void *host) {
     cudaError_t e = cudaFreeHost(host);
     return e == cudaSuccess ? 0 : cuda_fail(e, "cudaFreeHost");
+}
+
+int32_t mmffb_minimize_ctas(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt) {
+    int r = check_batch(batch, confs);
+    if (r) return r;
+    if (!opt) return fail(MMFFB_EINVAL, "null options");
+    Plan pl;
+    r = plan_minimize(batch, confs, opt, &pl);
+    return r ? r : pl.grid;
 }
 
 size_t mmffb_queue_scratch_bytes(const MMFFBatchDev *batch, const MMFFConfDev *confs, const MMFFOptParams *opt,

@@ -20,6 +20,7 @@ static int with_instance(const Plan &pl, bool lb, const Fn &fn) {
     }
     if (pl.nt == 64) return fn.template run<R, A, 64, 4, true, false>();
     if (pl.nt == 128) return fn.template run<R, A, 128, 8, true, false>();
+    if (pl.nc == 0) return fn.template run<R, A, 256, 0, true, false>();     // 128 registers, 2 CTAs/SM
     return fn.template run<R, A, 256, 8, true, false>();
 }
 

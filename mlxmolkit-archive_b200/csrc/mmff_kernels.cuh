@@ -1260,8 +1260,15 @@ struct Opt {
     }
 };
 
+// CTAs per SM a kernel instance is compiled for (its register budget): 2 for the
+// register-lean 256-thread instances (128 registers a thread), 1 otherwise.
+template <int NT, int NC, bool MSM>
+constexpr int min_ctas() {
+    return (NC == 0 && NT <= 256) || (MSM && NC <= 4 && NT == 256) ? 2 : 1;
+}
+
 template <class R, class A, int NT, int NC, bool MSM, bool LB>
-__global__ void __launch_bounds__(NT, (NC == 0 && NT <= 256) ? 2 : 1) minimize_kernel(const Params P) {
+__global__ void __launch_bounds__(NT, (min_ctas<NT, NC, MSM>())) minimize_kernel(const Params P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     __shared__ int s_abort;

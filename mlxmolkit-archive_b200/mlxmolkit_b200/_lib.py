@@ -124,7 +124,7 @@ DG_CONVERGED, DG_MAXIT = 0, 1
 
 EXPORTS = ["mmffb_version", "mmffb_last_error", "mmffb_energy_grad", "mmffb_fp64_check", "mmffb_minimize_scratch_bytes",
            "mmffb_minimize", "mmffb_plain_scratch_bytes", "mmffb_plain_minimize", "mmffb_fused_sd",
-           "mmffb_minimize_noalloc", "mmffb_queue_scratch_bytes", "mmffb_minimize_queue",
+           "mmffb_minimize_noalloc", "mmffb_minimize_ctas", "mmffb_queue_scratch_bytes", "mmffb_minimize_queue",
            "mmffb_host_alloc_mapped", "mmffb_host_free", "mmffb_pack_chunk", "mmffb_pack_begin", "mmffb_pack_finish", "mmffb_pack_free",
            "mmffb_multimol_hist_floats", "mmffb_multimol_step",
            "mmffb_dg_scratch_bytes", "mmffb_dg_minimize", "mmffb_dg_energy_grad",
@@ -197,6 +197,8 @@ def load():
                                           ctypes.POINTER(ctypes.c_void_p)]
     L.mmffb_host_free.restype = ctypes.c_int
     L.mmffb_host_free.argtypes = [P]
+    L.mmffb_minimize_ctas.restype = ctypes.c_int32
+    L.mmffb_minimize_ctas.argtypes = [BP, CP, OP]
     L.mmffb_queue_scratch_bytes.restype = ctypes.c_size_t
     L.mmffb_queue_scratch_bytes.argtypes = [BP, CP, OP, ctypes.c_int32]
     L.mmffb_minimize_queue.restype = ctypes.c_int

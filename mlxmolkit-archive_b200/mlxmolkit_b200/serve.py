@@ -231,6 +231,7 @@ class _Half:
         self.done_dev = self.done_buf.device_ptr
         self.workers: list = []                   # (end event, scratch index, launch time) of its launches
         self.pending: list = []                   # queue writes waiting for their data: (event, tail | None)
+        self.published = 0                        # the tail written last
         self.closed = True
         self.requests: list = []
         self.n_mol = self.n_row = self.n_atom = self.n_pair = self.n_word = self.n_slot = self.n_coord = 0
@@ -239,6 +240,7 @@ class _Half:
         """Empty the half for a new generation (no worker of it may be running)."""
         import torch
         self.n_mol = self.n_row = self.n_atom = self.n_pair = self.n_word = self.n_slot = self.n_coord = 0
+        self.published = 0
         self.done_np[:] = 0
         with torch.cuda.stream(stream):
             self.ctl.zero_()
@@ -266,7 +268,7 @@ class _Half:
 
     def live_workers(self) -> list:
         """Launches on this half that have not ended (ended ones are dropped)."""
-        self.workers = [w for w in self.workers if not w[0].query()]
+        self.workers = [w for w in self.workers if not w["ev"].query()]
         return self.workers
 
     def worker_running(self) -> bool:
@@ -278,6 +280,8 @@ class _Half:
 
 
 class _ClassState:
+    STREAMS = 16                  # concurrent worker launches per class at most
+
     def __init__(self, srv, key, cls: SizeClass, max_iters: int, caps: _Caps):
         torch = srv.torch
         self.key = key
@@ -286,30 +290,31 @@ class _ClassState:
         self.halves = [_Half(srv, caps), _Half(srv, caps)]
         self.cur = None
         self.copy_stream = torch.cuda.Stream(device=srv.device)
+        self.streams = [torch.cuda.Stream(device=srv.device) for _ in range(self.STREAMS)]
+        self.stream_busy = [None] * self.STREAMS       # end event of the launch on each stream
+        # the arenas were zeroed on the allocating stream: order every later use after it
+        self.copy_stream.wait_stream(torch.cuda.current_stream(srv.device))
         self.opt = mm.opt_params(max_iters, 1e-4, cls.history_m, "mixed")
-        h = self.halves[0]
-        bd, cd = self._descs(h)
-        need = srv.lib.mmffb_queue_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(self.opt), 0)
-        if need == 0:
-            _lib.check(_lib.MMFFB_EINVAL, "mmffb_queue_scratch_bytes")
-        # each concurrent worker launch needs its own scratch (work counter, error word, inverse-
-        # Hessian slots per CTA): up to MAX_WORKERS launches of the class at once, as a quarter
-        # of the budget allows
-        nw = int(max(1, min(self.MAX_WORKERS, (srv.budget // 4) // max(need, 1))))
-        self.scratch = [torch.empty(need, dtype=torch.uint8, device=srv.device) for _ in range(nw)]
-        self.scratch_busy = [None] * nw                # end event of the launch using it
-        self.compute_streams = [torch.cuda.Stream(device=srv.device) for _ in range(nw)]
-        self.nbytes = 2 * caps.nbytes() + nw * need
+        bd, cd = self._descs(self.halves[0])
+        self.full_grid = int(srv.lib.mmffb_minimize_ctas(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(self.opt)))
+        if self.full_grid <= 0:
+            _lib.check(self.full_grid or _lib.MMFFB_EINVAL, "mmffb_minimize_ctas")
+        self.slot_scratch = srv.lib.mmffb_queue_scratch_bytes(ctypes.byref(bd), ctypes.byref(cd),
+                                                              ctypes.byref(self.opt), 1) - 256
+        self.nbytes = 2 * caps.nbytes()
+        self.scratch_live: list = []                  # (end event, scratch tensor) of running launches
         self.launches = 0
 
-    MAX_WORKERS = 4
-
-    def free_scratch(self) -> Optional[int]:
-        for i, ev in enumerate(self.scratch_busy):
+    def free_stream(self) -> Optional[int]:
+        for i, ev in enumerate(self.stream_busy):
             if ev is None or ev.query():
-                self.scratch_busy[i] = None
+                self.stream_busy[i] = None
                 return i
         return None
+
+    def scratch_bytes_live(self) -> int:
+        self.scratch_live = [(ev, t) for ev, t in self.scratch_live if not ev.query()]
+        return sum(t.numel() for _, t in self.scratch_live)
 
     def _descs(self, h: _Half):
         c = h.caps
@@ -328,12 +333,17 @@ class MMFFServer:
 
     def __init__(self, hbm_budget_bytes: int = 8 << 30, prep_workers: int = 4, device=None,
                  default_max_iters: int = 1000, default_max_iters_lbfgs: int = 3000,
-                 max_slots_per_half: int = 4096, prep_cache_size: int = 4096, worker_idle_ms: float = 10.0):
-        """``worker_idle_ms``: a worker launch whose queue stays empty this long ends."""
+                 max_slots_per_half: int = 4096, prep_cache_size: int = 4096, worker_idle_ms: float = 1.0,
+                 min_worker_ctas: int = 0):
+        """``worker_idle_ms``: a worker CTA whose queue stays empty this long ends.
+        ``min_worker_ctas``: launch at least this many CTAs per worker (spare CTAs take slots
+        published while they wait)."""
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("MMFFServer needs a CUDA device")
         self.IDLE_POLLS = max(1, int(worker_idle_ms * 1e6 / self.SLEEP_NS))
+        self.idle_s = self.IDLE_POLLS * self.SLEEP_NS * 1e-9
+        self.min_worker_ctas = int(min_worker_ctas)
         self.torch = torch
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         self.budget = int(hbm_budget_bytes)
@@ -461,7 +471,7 @@ class MMFFServer:
         before its tables and coordinates are in device memory; the close flag after the tails."""
         torch = self.torch
         for h in cs.halves:
-            wrote = False
+            wrote = 0
             while h.pending:
                 ev, tail = h.pending[0]
                 if ev is not None and not ev.query():
@@ -472,11 +482,12 @@ class MMFFServer:
                         h.ctl[2:3].copy_(torch.ones(1, dtype=torch.int32).pin_memory(), non_blocking=True)
                     else:
                         h.ctl[1:2].copy_(torch.tensor([tail], dtype=torch.int32).pin_memory(), non_blocking=True)
-                        wrote = True
+                        wrote += tail - h.published
+                        h.published = tail
             if wrote:
                 ready = torch.cuda.Event()
                 ready.record(cs.copy_stream)
-                self._ensure_worker(cs, h, ready)
+                self._ensure_worker(cs, h, ready, wrote)
 
     def _publish(self, cs: _ClassState, h: _Half, reqs) -> None:
         """Copy the requests' tables, slot descriptors and coordinates into their reserved, contiguous
@@ -517,37 +528,52 @@ class MMFFServer:
             landed.record(cs.copy_stream)
         h.pending.append((landed, slot0 + len(conf_mol)))     # the new tail, once the data has landed
 
-    def _ensure_worker(self, cs: _ClassState, h: _Half, ready) -> None:
-        """Start a worker on h unless a recent one runs: a worker older than its idle limit may
-        have lost the CTAs that found the queue empty, so new slots get a fresh launch whose CTAs
-        take SMs as they free up (concurrent launches share the queue)."""
-        live = h.live_workers()
-        idle_s = self.IDLE_POLLS * self.SLEEP_NS * 1e-9
-        if live and time.perf_counter() - max(w[2] for w in live) < idle_s:
+    def _ensure_worker(self, cs: _ClassState, h: _Half, ready, new_slots: int) -> None:
+        """CTAs for ``new_slots`` just-published slots of h.  Spare CTAs of a launch younger than the
+        idle limit are still polling and take them first; the rest get a new launch sized to them
+        (at least ``min_worker_ctas``, at most the class's full grid).  Launches share the queue, so
+        whichever CTA frees up first takes the next slot."""
+        now = time.perf_counter()
+        for w in h.live_workers():
+            if new_slots <= 0:
+                return
+            if now - w["t"] < self.idle_s and w["spare"] > 0:
+                take = min(w["spare"], new_slots)
+                w["spare"] -= take
+                new_slots -= take
+        if new_slots <= 0:
             return
-        i = cs.free_scratch()
+        i = cs.free_stream()
         if i is None:
-            return                          # every scratch is in use: the running launches take the slots
-        self._launch_worker(cs, h, ready, i)
+            return                          # the running launches take the slots as CTAs free up
+        grid = int(min(cs.full_grid, max(new_slots, self.min_worker_ctas)))
+        per_cta = max(int(cs.slot_scratch), 0)
+        room = max(self.budget - self.in_use - cs.scratch_bytes_live(), 0)
+        if per_cta and 256 + grid * per_cta > room:
+            grid = int(max(1, min(grid, (room - 256) // per_cta)))
+        self._launch_worker(cs, h, ready, i, grid, 256 + grid * per_cta, grid - min(grid, new_slots))
 
-    def _launch_worker(self, cs: _ClassState, h: _Half, ready, i: int) -> None:
+    def _launch_worker(self, cs: _ClassState, h: _Half, ready, i: int, grid: int, scratch_bytes: int,
+                       spare: int) -> None:
         torch = self.torch
         L = self.lib
-        stream = cs.compute_streams[i]
+        stream = cs.streams[i]
         stream.wait_event(ready)
         bd, cd = cs._descs(h)
         q = _lib.MMFFQueueDev(h.ctl.data_ptr(), h.ctl.data_ptr() + 4, h.ctl.data_ptr() + 8, h.done_dev,
                               self.IDLE_POLLS, self.SLEEP_NS)
-        sc = cs.scratch[i]
+        with torch.cuda.stream(stream):
+            sc = torch.empty(scratch_bytes, dtype=torch.uint8, device=self.device)
         rc = L.mmffb_minimize_queue(ctypes.byref(bd), ctypes.byref(cd), ctypes.byref(cs.opt), ctypes.byref(q),
                                     h.pos.data_ptr(), h.energy.data_ptr(), h.status.data_ptr(),
-                                    h.iters.data_ptr(), 0, sc.data_ptr(), sc.numel(),
+                                    h.iters.data_ptr(), grid, sc.data_ptr(), sc.numel(),
                                     ctypes.c_void_p(stream.cuda_stream))
         _lib.check(rc, "mmffb_minimize_queue")
         ev = torch.cuda.Event()
         ev.record(stream)
-        h.workers.append((ev, i, time.perf_counter()))
-        cs.scratch_busy[i] = ev
+        h.workers.append({"ev": ev, "t": time.perf_counter(), "grid": grid, "spare": spare})
+        cs.stream_busy[i] = ev
+        cs.scratch_live.append((ev, sc))
         cs.launches += 1
         self.launches += 1
 
@@ -576,7 +602,7 @@ class MMFFServer:
             if keep and not h.pending and not h.worker_running():
                 ready = torch.cuda.Event()
                 ready.record(cs.copy_stream)
-                self._ensure_worker(cs, h, ready)
+                self._ensure_worker(cs, h, ready, sum(r.positions.shape[0] for r in keep))
 
     def _finish_copies(self) -> None:
         keep = []
@@ -672,7 +698,7 @@ class MMFFServer:
                     self._flush(cs)
                 for cs in self.classes.values():
                     cs.copy_stream.synchronize()
-                    for st in cs.compute_streams:
+                    for st in cs.streams:
                         st.synchronize()
                 break
             time.sleep(0.0002)

@@ -51,7 +51,8 @@ def test_requests_join_the_running_launch():
     free CTAs take their slots while the first request is still on the GPU."""
     from mlxmolkit_b200.serve import MMFFServer
     big, other = synth.make_molecules(2, [8, 2], 34, 64, 76, workers=1, max_atoms=260)   # L-BFGS class
-    srv = MMFFServer(hbm_budget_bytes=2 << 30, worker_idle_ms=3000.0)
+    # the first launch keeps 56 spare CTAs polling (64 CTAs for 8 conformers) for up to 3 s
+    srv = MMFFServer(hbm_budget_bytes=2 << 30, worker_idle_ms=3000.0, min_worker_ctas=64)
     f_big = srv.submit(big, max_iters=3000)
     time.sleep(0.01)
     f_other = srv.submit(other, max_iters=3000)
@@ -61,7 +62,11 @@ def test_requests_join_the_running_launch():
     srv.close()
     assert r_big.t_admit < r_other.t_admit < r_big.t_done      # admitted while the first one ran
     assert launches == {k: 1 for k in launches} and len(launches) == 1, launches
-    assert np.isfinite(r_big.energies).all() and np.isfinite(r_other.energies).all()
+    # and its result is the one it gets alone
+    srv = MMFFServer(hbm_budget_bytes=2 << 30)
+    alone = srv.submit(other, max_iters=3000).result(timeout=300)
+    srv.close()
+    assert np.array_equal(alone.energies, r_other.energies) and np.array_equal(alone.positions, r_other.positions)
 
 
 def test_requests_overlap_on_the_device():
