@@ -104,22 +104,8 @@ def _run_cpu(params, conf_mol, x, max_iters: int, history_m: int = 0, rdkit_cons
     return time.perf_counter() - t, e, st, oracle.max_threads(), xo
 
 
-# The FP64 minima a result is compared with run to convergence (the workloads' own caps stop some
-# FP64 runs early on the large molecules), with RDKit's optimizer constants.
-REF_CAP = 20000
-RULE = ("converged = final energy within 0.1 kcal/mol of an FP64 minimum: the one reached from the same "
-        "start (FP64, RDKit's optimizer constants, run to convergence), or the minimum of the basin the run "
-        "ended in (FP64 minimisation continued from the returned coordinates); two FP64 runs from one start "
-        "that differ only in rounding settle in different basins for some flexible molecules, so the "
-        "same-start comparison alone is not reproducible at 0.1 kcal/mol")
-
-
-def _converged(e, e_same, e_basin):
-    """The rule's mask and its parts (same start, own basin, one-sided against the same start)."""
-    same = np.abs(e - e_same) <= 0.1
-    basin = np.abs(e - e_basin) <= 0.1
-    return same | basin, {"same_start": float(same.mean()), "own_basin": float(basin.mean()),
-                          "one_sided_same_start": float(np.mean(e - e_same <= 0.1))}
+from mlxmolkit_b200.convergence import REF_CAP, RULE  # noqa: E402
+from mlxmolkit_b200.convergence import converged as _converged  # noqa: E402
 
 
 class _Clocks:
@@ -346,6 +332,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     from mlxmolkit_b200 import mmff_minimize as mm
+    from mlxmolkit_b200.convergence import fp64_minima
     from mlxmolkit_b200.replicas import rank_seed, reduce_step
     from mlxmolkit_b200.roofline import algorithmic_bytes
 
@@ -364,10 +351,7 @@ def main():
     # FP64 minima from the same starts (untimed): all-FP64 with RDKit's optimizer constants, run to
     # convergence -- the stand-in for RDKit's MMFFOptimizeMoleculeConfs
     def fp64_min(mn, x_dev):
-        y = x_dev.clone()
-        e_, st_, _ = mn.minimize_device(y, max_iters=REF_CAP, precision="fp64", consts=mm.RDKIT_CONSTS,
-                                        history_m=hist)
-        return e_.cpu().numpy()
+        return fp64_minima(mn, x_dev, hist)
 
     t64 = time.perf_counter()
     e64 = fp64_min(m, start)

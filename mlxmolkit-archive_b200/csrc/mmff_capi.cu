@@ -96,6 +96,13 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
             if (nt == 512) nt = 256;
             if (nt == 64 && n > 128) nt = 128;
             nc = nt == 64 ? 4 : 8;
+            // mixed precision with the CTA size left to the plan: the register-capped 256-thread
+            // instance (H columns read from shared memory, 128 registers, 2 CTAs and 16 warps per
+            // SM) -- the register-cached columns take 230 registers and leave 8 warps per SM
+            if (mixed && o->threads == 0) {
+                nt = 256;
+                nc = 0;
+            }
             if (nc > 0 && n > 32 * nc) msm = false;   // register-cached columns cover 32 * nc
         }
         if (!msm) {

@@ -1261,14 +1261,15 @@ struct Opt {
 };
 
 // CTAs per SM a kernel instance is compiled for (its register budget): 2 for the
-// register-lean 256-thread instances (128 registers a thread), 1 otherwise.
-template <int NT, int NC, bool MSM>
+// register-lean 256-thread dense BFGS instances (128 registers a thread, H columns
+// read from shared memory), 1 otherwise.
+template <int NT, int NC, bool MSM, bool LB>
 constexpr int min_ctas() {
-    return (NC == 0 && NT <= 256) || (MSM && NC <= 4 && NT == 256) ? 2 : 1;
+    return !LB && NC == 0 && NT <= 256 ? 2 : 1;
 }
 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>
-__global__ void __launch_bounds__(NT, (min_ctas<NT, NC, MSM>())) minimize_kernel(const Params P) {
+__global__ void __launch_bounds__(NT, (min_ctas<NT, NC, MSM, LB>())) minimize_kernel(const Params P) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     __shared__ int s_abort;

@@ -47,6 +47,12 @@ def run_rate(pool, rate: float, duration: float, budget: int, seed: int = 0) -> 
     t1 = time.perf_counter()
     srv.close()
     lat = np.array([r.latency for r in results])
+    atoms = np.array([r.positions.shape[1] for r in results])
+    per_class = {}
+    for name, sel in (("dense_bfgs_lt150_atoms", atoms < 150), ("lbfgs_150_atoms_up", atoms >= 150)):
+        if sel.any():
+            per_class[name] = {"requests": int(sel.sum()), "p50_ms": float(np.percentile(lat[sel], 50) * 1e3),
+                               "p99_ms": float(np.percentile(lat[sel], 99) * 1e3)}
     confs = sum(len(r.energies) for r in results)
     conv = sum(int(r.converged.sum()) for r in results)
     wall = t1 - t0
@@ -54,7 +60,8 @@ def run_rate(pool, rate: float, duration: float, budget: int, seed: int = 0) -> 
             "converged": conv, "wall_s": wall, "converged_per_s": conv / wall,
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "kept_up": bool(wall <= duration * 1.2 + 5.0), "peak_mem_bytes": int(srv.peak_in_use),
-            "launches": int(srv.launches), "mean_latency_ms": float(lat.mean() * 1e3)}
+            "launches": int(srv.launches), "mean_latency_ms": float(lat.mean() * 1e3), "per_class": per_class,
+            "converged_frac": conv / max(confs, 1)}
 
 
 def main():

@@ -205,3 +205,23 @@ def test_each_returned_energy_carries_its_fp64_check(golden, precision):
         assert r.energy_errors[c] == r.energies[c] - r.energies_fp64[c]
     tol = 1e-5 if precision == "mixed" else 1e-4
     assert np.all(np.abs(r.energy_errors) <= tol * np.maximum(1.0, np.abs(r.energies_fp64)))
+
+
+@pytest.mark.parametrize("lo,hi,threads", [(4, 8, 0), (10, 16, 0), (4, 8, 256), (10, 16, 128)])
+def test_shared_memory_instances_reach_the_fp64_minimum(lo, hi, threads):
+    """The inverse Hessian in shared memory, up to 24 and 25-48 atoms: the default register-capped
+    256-thread instance (threads=0) and the register-cached forms, against the FP64 oracle."""
+    mols, params, counts, pos = small_workload(n_mols=6, k=3, seed=81 + lo, lo=lo, hi=hi)
+    n = [p.n_atoms for p in params]
+    assert max(n) <= (24 if hi <= 8 else 48) and min(n) > (0 if hi <= 8 else 24), n
+    pos32 = pos.astype(np.float32)
+    m = mm.Minimizer(params, counts)
+    r = m.minimize(pos32, max_iters=2000, threads=threads)
+    _, eo, so, _ = oracle.minimize(params, counts, pos32.astype(np.float64), max_iters=4000,
+                                   consts=oracle.RDKIT_CONSTS)
+    d = np.abs(r.energies - eo)
+    assert np.mean(d <= 0.1) >= 0.9, d
+    assert r.converged.all(), r.status
+    assert np.all(np.abs(r.energy_errors) <= 1e-5 * np.maximum(1.0, np.abs(r.energies_fp64)))
+    r64 = m.minimize(pos32, max_iters=4000, precision="fp64", consts=mm.RDKIT_CONSTS, threads=threads)
+    assert np.mean(np.abs(r64.energies - eo) < 1e-3) >= 0.9
