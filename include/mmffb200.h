@@ -105,7 +105,8 @@ typedef struct {
                                     identity and continue, at most this many times per conformer */
     int32_t polish64;            /* MMFFB_PREC_MIXED: when the FP32 line-search energies stall (no
                                     Armijo decrease or a step below TOLX), continue with FP64 term
-                                    energies of the same FP32 coordinates for the line search */
+                                    energies of the same FP32 coordinates for the line search (the
+                                    Python host turns it on for L-BFGS and leaves it off for dense BFGS) */
     int32_t hpass_lean;          /* inverse Hessian in global memory: read its column vectors from
                                     shared memory instead of registers (2 CTAs per SM) */
     uint32_t wait_spins;         /* inverse Hessian in global memory: tests of a row copy's completion

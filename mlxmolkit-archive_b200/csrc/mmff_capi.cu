@@ -128,6 +128,17 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     };
     int fit = occupancy();
     if (fit < 0) return fit;
+    // mixed-precision L-BFGS with the history in shared memory: the register-capped instance
+    // (128 registers a thread) where two of its CTAs fit an SM by shared memory -- measured on
+    // the 150-170-atom class; where only one fits, the cap only adds spills (170-400 atoms
+    // measured 25 % slower)
+    if (mixed && lb && msm && o->threads == 0) {
+        pl->nc = 0;
+        const int fit2 = occupancy();
+        if (fit2 < 0) return fit2;
+        if (fit2 >= 2) fit = fit2;
+        else pl->nc = nc;
+    }
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
     int grid = sms * fit;
     if (grid > c->n_conf) grid = c->n_conf > 0 ? c->n_conf : 1;

@@ -11,8 +11,11 @@ template <class Fn>
 static int with_instance(const Plan &pl, bool lb, const Fn &fn) {
     using R = float;
     using A = double;
-    if (lb) return pl.msm ? fn.template run<R, A, 256, 2, true, true>()
-                          : fn.template run<R, A, 256, 2, false, true>();
+    if (lb) {
+        if (!pl.msm) return fn.template run<R, A, 256, 2, false, true>();
+        return pl.nc == 0 ? fn.template run<R, A, 256, 0, true, true>()     // 128 registers, 2 CTAs/SM
+                          : fn.template run<R, A, 256, 2, true, true>();
+    }
     if (!pl.msm) {
         if (pl.nc == 0) return pl.nt == 512 ? fn.template run<R, A, 512, 0, false, false>()
                                             : fn.template run<R, A, 256, 0, false, false>();

@@ -1262,10 +1262,11 @@ struct Opt {
 
 // CTAs per SM a kernel instance is compiled for (its register budget): 2 for the
 // register-lean 256-thread dense BFGS instances (128 registers a thread, H columns
-// read from shared memory), 1 otherwise.
+// read from shared memory) and for the register-capped L-BFGS instance (NC = 0,
+// history in shared memory), 1 otherwise.  For L-BFGS, NC only selects the budget.
 template <int NT, int NC, bool MSM, bool LB>
 constexpr int min_ctas() {
-    return !LB && NC == 0 && NT <= 256 ? 2 : 1;
+    return (!LB && NC == 0 && NT <= 256) || (LB && MSM && NC == 0 && NT == 256) ? 2 : 1;
 }
 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>

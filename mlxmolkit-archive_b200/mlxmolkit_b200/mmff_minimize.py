@@ -114,8 +114,11 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
                polish64: Optional[bool] = None, hpass_lean: bool = True, wait_spins: int = 0,
                err_word: int = 0, give_up_waits: bool = False) -> _lib.MMFFOptParams:
-    """Launch options; ``polish64`` (default: on for mixed precision) switches a conformer's
-    line-search energies to FP64 once the FP32 ones stall.  ``err_word``: device address of an
+    """Launch options; ``polish64`` switches a conformer's line-search energies to FP64 once the
+    FP32 ones stall.  Its default follows the optimizer: off for dense BFGS, whose mixed form is
+    then FP32 terms, gradients and update with FP64 only in the energy sums, the Armijo tests and
+    the convergence tests; on for mixed-precision L-BFGS, which on flexible 150-400-atom molecules
+    otherwise ends most conformers on an FP32 line-search stall short of the minimum.  ``err_word``: device address of an
     int32 that the launch sets to 1 when a bounded wait gives up; ``wait_spins`` bounds those
     waits (0: the library default); ``give_up_waits`` makes every such wait give up at once (a test
     switch that exercises the timeout path)."""
@@ -124,7 +127,7 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
     o.give_up_waits = int(bool(give_up_waits))
     o.err_word = int(err_word) or None
     o.max_restarts = int(max_restarts)
-    o.polish64 = int(precision == "mixed" if polish64 is None else bool(polish64))
+    o.polish64 = int(precision == "mixed" and history_m > 0 if polish64 is None else bool(polish64))
     o.hpass_lean = int(bool(hpass_lean))
     o.exit_test = int(exit_test)
     o.check_every = int(check_every)

@@ -4,8 +4,9 @@ Runs the same inputs three ways on the GPU:
 
 * ``fp64``  -- every term, gradient, vector and the inverse Hessian in FP64 (the GPU oracle);
 * ``mixed`` -- the chosen form: FP32 terms, gradients and BFGS update; FP64 energy sums,
-  Armijo comparisons and convergence tests; FP64 line-search energies once the FP32
-  ones stall;
+  Armijo comparisons and convergence tests;
+* ``mixed_fp64_polish`` -- the same, with FP64 line-search energies once the FP32 ones
+  stall (the L-BFGS default);
 * ``fp32``  -- everything FP32.
 
 For every conformer it reports |dE| against the FP64 minimum from the same start, whether it
@@ -42,7 +43,7 @@ def run(scale: float = 0.1, max_iters: int = 1000, seed: int = 0) -> dict:
     out = {}
     for name, kw in (("fp64", dict(precision="fp64", consts=mm.RDKIT_CONSTS)),
                      ("mixed", dict(precision="mixed")),
-                     ("mixed_no_fp64_polish", dict(precision="mixed", polish64=False)),
+                     ("mixed_fp64_polish", dict(precision="mixed", polish64=True)),
                      ("fp32", dict(precision="fp32"))):
         x = start.clone()
         torch.cuda.synchronize()

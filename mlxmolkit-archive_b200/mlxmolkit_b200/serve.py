@@ -18,10 +18,11 @@ time.  The service
   memory, copies each finished request's results back and completes its
   future.
 
-A worker whose queue stays empty for 10 ms ends (every wait in the kernel is
-bounded) and frees its SMs for the other classes; new slots start a new
-launch when the newest one is older than that, and several launches may share
-a queue.  A half is filled in order and refilled only when its worker
+A worker CTA whose queue stays empty for ``worker_idle_ms`` (1 ms by default)
+ends (every wait in the kernel is bounded) and frees its SM for the other
+classes.  New slots go first to spare CTAs of a launch younger than that limit
+and otherwise start a new launch sized to them; several launches may share a
+queue.  A half is filled in order and refilled only when its worker
 launches have ended and its requests are complete, so no running launch ever
 reads memory written after it started; the other half takes the requests
 meanwhile.  Device memory is bounded by the budget: arenas and worker scratch
