@@ -459,7 +459,8 @@ def mmff_minimize_nk(
     use_lbfgs: bool = False,
     return_result: bool = False,
 ):
-    """Minimise N molecules x k conformers on the GPU (one persistent launch per size class).
+    """Minimise N molecules x k conformers on the GPU (persistent launches per size class,
+    pipelined behind the packing: ``minimize_pipelined``).
 
     Same signature and return values as the reference
     (mlxmolkit/mmff_minimize.py:231-346): ``positions_3d`` is the flat
@@ -472,14 +473,137 @@ def mmff_minimize_nk(
     check (FP64 energy at the returned coordinates, the returned energy's error
     against it, FP64 RMS gradient) and the host time of each step.
     """
-    t0 = time.perf_counter()
-    m = BinnedMinimizer(mmff_params_list, conf_counts, tuning=load_tuning())
-    t1 = time.perf_counter()
-    r = m.minimize(positions_3d, max_iters=max_iters, grad_tol=grad_tol,
-                   history_m=LBFGS_M if use_lbfgs else 0)
-    t2 = time.perf_counter()
+    r = minimize_pipelined(mmff_params_list, conf_counts, positions_3d, max_iters=max_iters,
+                           grad_tol=grad_tol, history_m=LBFGS_M if use_lbfgs else 0)
     if not return_result:
         return r.positions, r.energies.astype(np.float32), r.converged
-    r.timings = {"setup_s": t1 - t0, "pack_s": m.pack_s, "minimize_s": t2 - t1, "total_s": t2 - t0,
-                 "upload_bytes": int(m.upload_bytes)}
     return r.positions, r.energies.astype(np.float32), r.converged, r
+
+
+_CHUNK_STREAMS: dict = {}
+
+
+def _chunk_stream(device, r: int):
+    """The stream of launch position r on ``device``: the same streams on every call, so the
+    caching allocator reuses each position's scratch blocks (it keeps freed blocks per stream);
+    priority highest for r = 0 and one level lower per position, down to the lowest."""
+    torch = _torch()
+    key = (str(device), r)
+    s = _CHUNK_STREAMS.get(key)
+    if s is None:
+        lowest, highest = torch.cuda.Stream.priority_range()
+        s = torch.cuda.Stream(device=device, priority=min(lowest, highest + r))
+        _CHUNK_STREAMS[key] = s
+    return s
+
+
+def _ranges(starts, lens) -> np.ndarray:
+    """The concatenated index ranges [starts[i], starts[i] + lens[i])."""
+    starts = np.asarray(starts, dtype=np.int64)
+    lens = np.asarray(lens, dtype=np.int64)
+    if lens.size == 0:
+        return np.zeros(0, dtype=np.int64)
+    first = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    return np.repeat(starts - first, lens) + np.arange(int(lens.sum()), dtype=np.int64)
+
+
+def launch_chunks(n_atoms, conf_counts, bins=DEFAULT_BINS, head_frac: float = 0.2, min_split: int = 64):
+    """Molecule index groups of a pipelined call, in launch order.
+
+    Molecules with conformers are grouped by size class (``bins``, as ``BinnedMinimizer``;
+    atom counts above the last bound form a class of their own), largest class first and
+    largest molecules first within a class.  The first class is split after its largest
+    ``head_frac`` of molecules (when it has at least ``min_split``), so the first launch
+    waits only for their packing.
+    """
+    n = np.asarray(n_atoms, dtype=np.int64)
+    k = np.asarray(conf_counts, dtype=np.int64)
+    live = np.nonzero(k > 0)[0]
+    cls = np.searchsorted(np.asarray(bins, dtype=np.int64), n[live], side="left")
+    chunks = []
+    for c in sorted(set(cls.tolist()), reverse=True):
+        mols = live[cls == c]
+        mols = mols[np.lexsort((mols, -n[mols]))]
+        if not chunks and len(mols) >= min_split:
+            h = max(1, int(math.ceil(head_frac * len(mols))))
+            chunks += [mols[:h], mols[h:]]
+        else:
+            chunks.append(mols)
+    return chunks
+
+
+def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, grad_tol: float = 1e-4,
+                       history_m: int = 0, device=None) -> MinimizeResult:
+    """The drop-in call's body: pack, upload and launch chunk by chunk (``launch_chunks``).
+
+    Chunk r is packed (native, host threads), uploaded and launched on its own stream while
+    the GPU runs chunks 0..r-1; streams get priorities in launch order, so a later chunk's
+    CTAs take SMs as an earlier chunk's work queue drains.  The call returns after its last
+    chunk's results are on the host.  Each chunk's FP64 check and
+    result copies follow its launch on the same stream.  A conformer's result depends only
+    on the kernel instance of its size class, so it is the same as in one ``BinnedMinimizer``
+    launch per class.  ``timings`` holds host seconds: ``setup_s`` until the first launch,
+    ``pack_s`` over all chunks (mostly overlapped), ``minimize_s`` from the first launch to the
+    last result, ``total_s``.
+    """
+    torch = _torch()
+    t0 = time.perf_counter()
+    params_list = list(params_list)
+    k = np.asarray([int(c) for c in conf_counts], dtype=np.int64)
+    n = np.asarray([int(p.n_atoms) for p in params_list], dtype=np.int64)
+    if len(k) != len(params_list):
+        raise ValueError("conf_counts needs one entry per molecule")
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    sizes = 3 * n * k
+    coord0 = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    conf0 = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+    if pos.size != int(coord0[-1]):
+        raise ValueError(f"positions hold {pos.size} floats, the conformers need {int(coord0[-1])}")
+    C = int(conf0[-1])
+    chunks = launch_chunks(n, k)
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    live = []
+    pack_s, upload, t_first = 0.0, 0, None
+    for r, idx in enumerate(chunks):
+        s = _chunk_stream(dev, r)
+        with torch.cuda.stream(s):
+            m = Minimizer([params_list[i] for i in idx], [int(k[i]) for i in idx], dev)
+            pack_s += m.pack_s
+            xh = torch.from_numpy(np.concatenate([pos[coord0[i]:coord0[i + 1]] for i in idx])).pin_memory()
+            x = torch.empty(xh.numel(), dtype=torch.float32, device=dev)
+            x.copy_(xh, non_blocking=True)
+            err = torch.zeros(1, dtype=torch.int32, device=dev)
+            e, st, it = m.minimize_device(x, max_iters=max_iters, grad_tol=grad_tol, history_m=history_m,
+                                          err=err, stream=s)
+            if t_first is None:
+                t_first = time.perf_counter()
+            e64, de, gr = m.fp64_check_device(x, e, stream=s)
+            host = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in (x, e, st, it, e64, de, gr, err)]
+            for h, t in zip(host, (x, e, st, it, e64, de, gr, err)):
+                h.copy_(t, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(s)
+        upload += m.upload_bytes          # tables and conformer index arrays (coordinates apart)
+        live.append((idx, m, done, host, (x, e, st, it, e64, de, gr, err)))
+    out_pos = np.empty(pos.size, dtype=np.float32)
+    outs = [np.empty(C, dtype=np.float64), np.empty(C, dtype=np.int32), np.empty(C, dtype=np.int32),
+            np.empty(C, dtype=np.float64), np.empty(C, dtype=np.float64), np.empty(C, dtype=np.float64)]
+    gave_up, bad = False, 0
+    for idx, m, done, host, _ in live:
+        done.synchronize()
+        hx, he, hst, hit, he64, hde, hgr, herr = (h.numpy() for h in host)
+        out_pos[_ranges(coord0[idx], sizes[idx])] = hx
+        cidx = _ranges(conf0[idx], k[idx])
+        for o, h in zip(outs, (he, hst, hit, he64, hde, hgr)):
+            o[cidx] = h
+        if int(herr[0]):
+            gave_up = True
+            bad += int(np.sum(hst == _lib.ST_TIMEOUT))
+    if gave_up:
+        raise _lib.MMFFBError("mmffb_minimize: a bounded wait inside the kernel gave up; "
+                              f"{bad} conformers have no valid result")
+    t2 = time.perf_counter()
+    res = MinimizeResult(out_pos, *outs)
+    res.timings = {"setup_s": (t_first or t2) - t0, "pack_s": pack_s, "minimize_s": t2 - (t_first or t2),
+                   "total_s": t2 - t0, "upload_bytes": int(upload), "launch_chunks": len(chunks)}
+    return res

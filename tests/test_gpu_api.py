@@ -130,6 +130,28 @@ def test_mmff_minimize_nk_drop_in():
     assert np.isfinite(e2).all() and conv2.mean() >= 0.5
 
 
+def test_pipelined_call_equals_one_launch_per_size_class():
+    """mmff_minimize_nk packs and launches chunk by chunk (the largest molecules first, their
+    class split in two); every conformer's result is bit-identical to BinnedMinimizer's one
+    launch per size class, in the caller's conformer order, zero-conformer molecules included."""
+    mols = synth.make_molecules(130, 2, 75, 6, 50, workers=1, max_atoms=150)
+    params = [extract_mmff_params(m) for m in mols]
+    counts = [0 if i == 7 else 2 for i in range(len(mols))]
+    pos = np.concatenate([np.stack([c.pos for c in m.GetConformers()][:k]).reshape(-1)
+                          for m, k in zip(mols, counts) if k]).astype(np.float32)
+    n = np.array([p.n_atoms for p in params])
+    chunks = mm.launch_chunks(n, counts)
+    assert len(chunks) == 4 and 7 not in np.concatenate(chunks)     # 49-150 atoms split in two
+    x, e, conv, r = mm.mmff_minimize_nk(params, counts, pos, max_iters=300, return_result=True)
+    assert r.timings["launch_chunks"] == len(chunks)
+    b = mm.BinnedMinimizer(params, counts).minimize(pos, max_iters=300)
+    assert np.array_equal(x, b.positions)
+    assert np.array_equal(r.energies, b.energies)
+    assert np.array_equal(r.status, b.status) and np.array_equal(r.iters, b.iters)
+    assert np.array_equal(r.energies_fp64, b.energies_fp64)
+    assert np.array_equal(conv, b.converged)
+
+
 def test_generate_conformers_nk_runs_the_mmff_stage():
     from mlxmolkit_b200.conformer_pipeline_v2 import generate_conformers_nk
     mols = synth.make_molecules(3, 3, 73, 8, 20, workers=1)
