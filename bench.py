@@ -46,8 +46,8 @@ UNIT = "conformers/s"
 WORKLOADS = {
     "druglike": "druglike: 2000 mols x 10 confs, heavy 8-70 (20-150 atoms), MMFF94/94s 50/50, dense BFGS, max 1000 it",
     "small": "small: 50 mols x 50 confs, heavy 10-30, MMFF94, dense BFGS, max 2000 it",
-    "large": "large: 500 mols x 8 confs, heavy 60-160 (150-400 atoms), 30% with a 12-18 macrocycle, <= 20 "
-             "rotatable bonds, MMFF94, L-BFGS m=8, max 3000 it",
+    "large": "large: 500 mols x 8 confs, heavy atoms uniform on 60-160 (with H about 130-370 atoms), 30% with "
+             "a 12-18 macrocycle, <= 20 rotatable bonds, MMFF94, L-BFGS m=8, max 3000 it",
     "dg": "dg: the distance-geometry stage (4-D L-BFGS + 200-iteration collapse) of 20 mols x 50 confs, "
           "heavy 10-30, metric-matrix starts, budget max(300, 300 + 20 * complexity)",
 }
@@ -395,6 +395,17 @@ def main():
     conv = int(mask.sum())
     ms_step, conv_all = reduce_step(dist, float(np.mean(times)), conv, dev)
     value = conv_all / (ms_step / 1e3)
+    # below the 98 % target: the same algorithm in FP64 under the same iteration cap (untimed),
+    # which tells whether the shortfall is the optimizer's at this cap or the precision's
+    same_cap = None
+    if conv / C < 0.98:
+        x64 = start.clone()
+        e_cap, st_cap, _ = m.minimize_device(x64, max_iters=wl.max_iters, history_m=hist, precision="fp64")
+        m64, _ = _converged(e_cap.cpu().numpy(), e64, fp64_min(m, x64))
+        same_cap = {"converged_frac": float(m64.mean()), "max_iters": wl.max_iters,
+                    "at_cap": int((st_cap == 1).sum().item()),
+                    "what": "the same optimizer and constants in FP64 with the same iteration cap, judged by "
+                            "the same rule"}
 
     # end to end through the drop-in call mmff_minimize_nk (mlxmolkit/mmff_minimize.py:231-346), from
     # host arrays to host arrays: native packing of the tables, their upload and the coordinates',
@@ -497,8 +508,11 @@ def main():
             "data": "synthetic (seeded RDKit-free generator; RDKit absent)",
             "config": {"workload": WORKLOADS[a.workload] + ("" if a.scale == 1.0 else f" x scale {a.scale}"),
                        "molecules": len(params), "conformers": C, "parallelism": f"dp{world} (replicas)",
+                       "atoms": [int(min(p.n_atoms for p in params)), int(max(p.n_atoms for p in params))],
+                       "mean_atoms": float(np.mean([p.n_atoms for p in params])),
                        "l2": "flushed (256 MB write) between timed steps"},
             "converged_frac": conv / C, "converged_rule": RULE, "converged_parts": parts,
+            "target_met": bool(conv / C >= 0.98), "fp64_same_cap": same_cap,
             "mean_abs_dE_same_start": float(dE.mean()), "fp64_reference_s": t64, "prep_s": t_prep,
             "iters_mean": float(it_mix.mean()), "ls_evals_mean": float(ev.mean()),
             "status_counts": np.bincount(st_mix, minlength=6).tolist(),

@@ -85,7 +85,9 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     if (!lb && n > 512) return fail(MMFFB_ETOOBIG, "dense BFGS supports up to 170 atoms (got %d); use L-BFGS", nmax);
     const int mc = b->max_classes;
     if (nt == 512 && (lb || !mixed)) nt = 256;
-    Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as, mc);
+    // L-BFGS decides from the atom bound alone (the full 64-entry class table), so that every
+    // launch of one atom bound -- whatever its molecules' class counts -- runs the same instance
+    Layout Ls = make_layout(nmax, nt / 32, o->history_m, true, rs, as, lb ? 64 : mc);
     bool msm = Ls.total <= (size_t)optin;
     // mixed-precision dense BFGS above 48 atoms: the register-lean streamed instance (H in a
     // global slot, 2 CTAs/SM) beats a shared-memory H that leaves one CTA of 8 warps per SM
@@ -131,13 +133,21 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     // mixed-precision L-BFGS with the history in shared memory: the register-capped instance
     // (128 registers a thread) where two of its CTAs fit an SM by shared memory -- measured on
     // the 150-170-atom class; where only one fits, the cap only adds spills (170-400 atoms
-    // measured 25 % slower)
+    // measured 25 % slower).  Decided at the atom bound with a 32-entry class table (the
+    // serving classes' bound), so the instance does not depend on the launch's molecules; a
+    // launch whose tables are larger still runs, with the CTAs that fit.
     if (mixed && lb && msm && o->threads == 0) {
         pl->nc = 0;
+        pl->smem = make_layout(nmax, nt / 32, o->history_m, true, rs, as, 32).total;
         const int fit2 = occupancy();
+        pl->smem = L.total;
         if (fit2 < 0) return fit2;
-        if (fit2 >= 2) fit = fit2;
-        else pl->nc = nc;
+        if (fit2 >= 2) {
+            fit = occupancy();
+            if (fit < 0) return fit;
+        } else {
+            pl->nc = nc;
+        }
     }
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
     int grid = sms * fit;

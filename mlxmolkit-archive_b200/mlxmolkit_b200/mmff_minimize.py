@@ -540,9 +540,9 @@ def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, g
     the GPU runs chunks 0..r-1; streams get priorities in launch order, so a later chunk's
     CTAs take SMs as an earlier chunk's work queue drains.  The call returns after its last
     chunk's results are on the host.  Each chunk's FP64 check and
-    result copies follow its launch on the same stream.  A conformer's result depends only
-    on the kernel instance of its size class, so it is the same as in one ``BinnedMinimizer``
-    launch per class.  ``timings`` holds host seconds: ``setup_s`` until the first launch,
+    result copies follow its launch on the same stream.  Every chunk is planned at its size
+    class's atom bound, and the planner picks the kernel instance from the atom bound alone,
+    so a conformer's result is the same as in one ``BinnedMinimizer`` launch per class.  ``timings`` holds host seconds: ``setup_s`` until the first launch,
     ``pack_s`` over all chunks (mostly overlapped), ``minimize_s`` from the first launch to the
     last result, ``total_s``.
     """
@@ -561,6 +561,12 @@ def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, g
         raise ValueError(f"positions hold {pos.size} floats, the conformers need {int(coord0[-1])}")
     C = int(conf0[-1])
     chunks = launch_chunks(n, k)
+    # every chunk is planned at its size class's atom bound (the largest molecule of the class),
+    # as the class's one launch in BinnedMinimizer is: the same kernel instance and layout
+    cls_of = [int(np.searchsorted(np.asarray(DEFAULT_BINS), n[c[0]], side="left")) for c in chunks]
+    bound = {}
+    for c, ci in zip(chunks, cls_of):
+        bound[ci] = max(bound.get(ci, 0), int(n[c].max()))
     dev = device or torch.device("cuda", torch.cuda.current_device())
     live = []
     pack_s, upload, t_first = 0.0, 0, None
@@ -568,6 +574,7 @@ def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, g
         s = _chunk_stream(dev, r)
         with torch.cuda.stream(s):
             m = Minimizer([params_list[i] for i in idx], [int(k[i]) for i in idx], dev)
+            m.confs.max_atoms = bound[cls_of[r]]
             pack_s += m.pack_s
             xh = torch.from_numpy(np.concatenate([pos[coord0[i]:coord0[i + 1]] for i in idx])).pin_memory()
             x = torch.empty(xh.numel(), dtype=torch.float32, device=dev)

@@ -41,12 +41,16 @@ is bit-for-bit the same alone or in any mix of requests.
 | 25-48   | dense BFGS  | 48         | 64                |
 | 49-149  | dense BFGS  | 149        | 32                |
 | 49-149 with more than 32 non-bonded classes | dense BFGS | 149 | 64 |
-| 150-300 | L-BFGS m=8  | 300        | 64                |
+| 150-170 | L-BFGS m=8  | 170        | 32                |
+| 150-170 with more than 32 non-bonded classes | L-BFGS m=8 | 170 | 64 |
+| 171-300 | L-BFGS m=8  | 300        | 64                |
 | 301-400 | L-BFGS m=8  | 400        | 64                |
 | > 400   | L-BFGS m=8  | its own    | 64                |
 
 Molecules of 150 atoms or more use L-BFGS, as in the reference pipeline
-(mlxmolkit/conformer_pipeline_v2.py:448-452), decided per molecule.
+(mlxmolkit/conformer_pipeline_v2.py:448-452), decided per molecule.  The
+150-170-atom L-BFGS class keeps its launch shape small (32 class-table
+entries) so that its instance fits two CTAs per SM, the register-capped one.
 """
 from __future__ import annotations
 
@@ -95,6 +99,10 @@ class SizeClass:
 def size_class(n_atoms: int, n_classes: int) -> SizeClass:
     """The launch class of a molecule (a function of its own atom and class counts)."""
     if n_atoms >= mm.LBFGS_ATOM_THRESHOLD:
+        if n_atoms <= 170:
+            if n_classes > 32:
+                return SizeClass(("lbfgs", 170, 64), 170, 64, mm.LBFGS_M)
+            return SizeClass(("lbfgs", 170), 170, 32, mm.LBFGS_M)
         if n_atoms <= 300:
             return SizeClass(("lbfgs", 300), 300, 64, mm.LBFGS_M)
         if n_atoms <= 400:

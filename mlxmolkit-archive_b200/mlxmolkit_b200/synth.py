@@ -327,25 +327,45 @@ def generate_molecule(rng: np.random.Generator, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macrocycle: bool = False,
                       max_rotatable: int | None = None, name: str = "",
                       max_tries: int = 50, max_atoms: int | None = None,
-                      ring_density: float = 0.0) -> SynthMol:
+                      ring_density: float = 0.0, keep_target: bool = False) -> SynthMol:
     """Grow one seeded drug-like molecule (explicit H) of heavy_lo..heavy_hi heavy atoms.
 
     Draws that exceed max_rotatable rotatable bonds or max_atoms atoms (with H)
-    are rejected and redrawn.
+    are rejected and redrawn.  With ``keep_target`` the size comes first: the
+    heavy-atom count is drawn once (uniform on heavy_lo..heavy_hi) and kept across
+    redraws, and each draw rejected for its rotatable bonds raises the ring density
+    by a fifth and grows the next one more rigidly (new atoms onto ring atoms rather
+    than chain ends); when no draw meets max_rotatable the least flexible one is kept
+    (rings attach through single bonds here, so a large skeleton cannot always stay
+    under the limit).
     """
+    target = int(rng.integers(heavy_lo, heavy_hi + 1)) if keep_target else None
+    density = ring_density
+    rigid = 0.0
+    best, best_rot = None, None
     for _ in range(max_tries):
-        mol = _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_density)
+        lo, hi = (target, target) if keep_target else (heavy_lo, heavy_hi)
+        mol = _try_generate(rng, lo, hi, max_rings, macrocycle, name, density, rigid)
         if mol is None:
-            continue
-        if max_rotatable is not None and count_rotatable(mol) > max_rotatable:
             continue
         if max_atoms is not None and mol.GetNumAtoms() > max_atoms:
             continue
+        if max_rotatable is not None:
+            rot = count_rotatable(mol)
+            if rot > max_rotatable:
+                if keep_target:
+                    density = min(0.3, max(density, 0.05) * 1.2)
+                    rigid = min(0.95, rigid + 0.25)
+                    if best is None or rot < best_rot:
+                        best, best_rot = mol, rot
+                continue
         return mol
+    if best is not None:
+        return best
     raise RuntimeError("molecule generation failed repeatedly")
 
 
-def _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_density=0.0):
+def _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_density=0.0, rigid=0.0):
     target = int(rng.integers(heavy_lo, heavy_hi + 1))
     if ring_density > 0:
         # ring-rich large molecules: about one ring per 1/ring_density heavy atoms
@@ -377,6 +397,10 @@ def _try_generate(rng, heavy_lo, heavy_hi, max_rings, macrocycle, name, ring_den
         # drug-like skeletons grow mostly as chains: weight sites against branching
         hdeg = np.array([sum(1 for (i, j, _) in sk.bonds if a_ in (i, j)) for a_ in sites], float)
         w = 1.0 / (1.0 + hdeg ** 3)
+        if rigid > 0:
+            # rigid growth: new atoms go mostly onto ring atoms, as terminal substituents or
+            # linked rings, rather than extending chains (no new rotatable bonds)
+            w = np.where(np.array([sk.ring[a_] >= 0 for a_ in sites]), 1.0, w * (1.0 - rigid))
         a = sites[int(rng.choice(len(sites), p=w / w.sum()))]
         room = target - sk.heavy()
         if ring_plan and room >= ring_plan[-1][0] and rng.random() < 0.35:
@@ -1054,14 +1078,15 @@ class Workload:
 def make_one_molecule(seed: int, m: int, k: int, heavy_lo: int, heavy_hi: int,
                       max_rings: int = 3, macro_frac: float = 0.0,
                       max_rotatable: int | None = None, noise: float = 0.1,
-                      max_atoms: int | None = None, ring_density: float = 0.0) -> SynthMol:
+                      max_atoms: int | None = None, ring_density: float = 0.0,
+                      keep_target: bool = False) -> SynthMol:
     """Molecule m of the seeded stream: its own generator seeded by (seed, m)."""
     rng = np.random.default_rng([seed, m])
     macro = macro_frac > 0 and rng.random() < macro_frac
     mol = generate_molecule(rng, heavy_lo, heavy_hi, max_rings=max_rings,
                             macrocycle=macro, max_rotatable=max_rotatable,
                             name=f"synth-{seed}-{m}", max_atoms=max_atoms, ring_density=ring_density,
-                            max_tries=200)
+                            max_tries=40 if keep_target else 200, keep_target=keep_target)
     for c in embed_conformers(mol, int(k), rng, noise=noise):
         mol.AddConformer(c)
     return mol
@@ -1074,7 +1099,8 @@ def _make_one_star(args):
 def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_hi: int,
                    max_rings: int = 3, macro_frac: float = 0.0,
                    max_rotatable: int | None = None, noise: float = 0.1,
-                   workers: int | None = None, max_atoms: int | None = None, ring_density: float = 0.0):
+                   workers: int | None = None, max_atoms: int | None = None, ring_density: float = 0.0,
+                   keep_target: bool = False):
     """n_mols seeded molecules, each with k (or k[i]) embedded noisy conformers.
 
     Each molecule has its own generator seeded by (seed, index), so the result
@@ -1084,7 +1110,7 @@ def make_molecules(n_mols: int, k: int | list, seed: int, heavy_lo: int, heavy_h
     ks = [int(k[m]) if isinstance(k, (list, tuple, np.ndarray)) else int(k)
           for m in range(n_mols)]
     jobs = [(seed, m, ks[m], heavy_lo, heavy_hi, max_rings, macro_frac, max_rotatable, noise, max_atoms,
-             ring_density) for m in range(n_mols)]
+             ring_density, keep_target) for m in range(n_mols)]
     if workers is None:
         workers = min(os.cpu_count() or 1, 16) if n_mols >= 64 else 1
     if workers <= 1:
@@ -1110,8 +1136,9 @@ def make_workload(name: str, seed: int = 0, scale: float = 1.0) -> Workload:
     * ``small``:    50 molecules x 50 conformers, heavy atoms 10-30, MMFF94, at most 2000 iterations;
     * ``druglike``: 2000 molecules x 10 conformers, heavy atoms 8-70 (at most 150 atoms),
       MMFF94 / MMFF94s alternating, dense BFGS, at most 1000 iterations;
-    * ``large``:    500 molecules x 8 conformers, heavy atoms 60-160 (at most 400 atoms),
-      30 % macrocycles, at most 20 rotatable bonds, L-BFGS, at most 3000 iterations.
+    * ``large``:    500 molecules x 8 conformers, heavy atoms uniform on 60-160 (at most 400
+      atoms), 30 % macrocycles, at most 20 rotatable bonds where the skeleton allows it (else
+      the least flexible of 40 draws), L-BFGS, at most 3000 iterations.
     """
     def n(x):
         return max(1, int(round(x * scale)))
@@ -1124,6 +1151,6 @@ def make_workload(name: str, seed: int = 0, scale: float = 1.0) -> Workload:
         return Workload("druglike-2000x10-heavy8-70", mols, var, 1000, False)
     if name == "large":
         mols = make_molecules(n(500), 8, seed, 60, 160, macro_frac=0.3, max_rotatable=20, max_atoms=400,
-                              ring_density=0.12)
+                              ring_density=0.12, keep_target=True)
         return Workload("large-500x8-heavy60-160", mols, ["MMFF94"] * len(mols), 3000, True)
     raise ValueError(f"unknown workload {name!r}; one of {WORKLOADS}")

@@ -150,6 +150,12 @@ def test_pipelined_call_equals_one_launch_per_size_class():
     assert np.array_equal(r.status, b.status) and np.array_equal(r.iters, b.iters)
     assert np.array_equal(r.energies_fp64, b.energies_fp64)
     assert np.array_equal(conv, b.converged)
+    # L-BFGS: the planner picks its instance (history in shared memory or not, register-capped
+    # or not) from the class's atom bound, so the chunk of smaller molecules runs the same one
+    x, e, conv, r = mm.mmff_minimize_nk(params, counts, pos, max_iters=300, use_lbfgs=True, return_result=True)
+    b = mm.BinnedMinimizer(params, counts).minimize(pos, max_iters=300, history_m=mm.LBFGS_M)
+    assert np.array_equal(x, b.positions) and np.array_equal(r.energies, b.energies)
+    assert np.array_equal(r.status, b.status) and np.array_equal(r.iters, b.iters)
 
 
 def test_generate_conformers_nk_runs_the_mmff_stage():
