@@ -507,7 +507,7 @@ def _ranges(starts, lens) -> np.ndarray:
     return np.repeat(starts - first, lens) + np.arange(int(lens.sum()), dtype=np.int64)
 
 
-def launch_chunks(n_atoms, conf_counts, bins=DEFAULT_BINS, head_frac: float = 0.2, min_split: int = 64):
+def launch_chunks(n_atoms, conf_counts, bins=DEFAULT_BINS, head_frac: float = 0.1, min_split: int = 64):
     """Molecule index groups of a pipelined call, in launch order.
 
     Molecules with conformers are grouped by size class (``bins``, as ``BinnedMinimizer``;
