@@ -136,17 +136,29 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
     // measured 25 % slower).  Decided at the atom bound with a 32-entry class table (the
     // serving classes' bound), so the instance does not depend on the launch's molecules; a
     // launch whose tables are larger still runs, with the CTAs that fit.
-    if (mixed && lb && msm && o->threads == 0) {
-        pl->nc = 0;
-        pl->smem = make_layout(nmax, nt / 32, o->history_m, true, rs, as, 32).total;
-        const int fit2 = occupancy();
-        pl->smem = L.total;
-        if (fit2 < 0) return fit2;
-        if (fit2 >= 2) {
+    if (mixed && lb && o->threads == 0) {
+        // the register-capped instance with the history where it is: in shared memory if two
+        // CTAs fit so, else in a global slot if two fit that way (up to about 290 atoms; the
+        // slots of a full grid take a few tens of MB, L2-resident), else the uncapped one
+        bool capped = false;
+        for (int where = msm ? 1 : 0; where >= 0 && !capped; --where) {
+            pl->nc = 0;
+            pl->msm = where == 1;
+            pl->smem = make_layout(nmax, nt / 32, o->history_m, where == 1, rs, as, 32).total;
+            const int fit2 = occupancy();
+            if (fit2 < 0) return fit2;
+            capped = fit2 >= 2;
+        }
+        if (capped) {
+            msm = pl->msm;
+            L = make_layout(nmax, nt / 32, o->history_m, msm, rs, as, mc);
+            pl->smem = L.total;
             fit = occupancy();
             if (fit < 0) return fit;
         } else {
             pl->nc = nc;
+            pl->msm = msm;
+            pl->smem = L.total;
         }
     }
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;

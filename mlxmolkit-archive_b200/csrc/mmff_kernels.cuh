@@ -815,16 +815,12 @@ struct Opt {
     // rows of H and the vectors are padded to a multiple of 4 with zeros) and two
     // rows per step, so each vector load from shared memory serves two rows and a
     // warp keeps two row copies of its TMA ring in use at once.
-    // rev: this warp's rows in descending order.  Passes alternate direction, so each pass
-    // starts on the rows the previous one wrote last, the likeliest still in L2 (the CTAs'
-    // slots together exceed it).  A row's arithmetic does not depend on the order.
-    __device__ __forceinline__ void hpass_stream_v4(bool pending, bool rev) {
+    __device__ __forceinline__ void hpass_stream_v4(bool pending) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const int ldr = hld(3 * P.nmax);
         float *rw = (float *)ring + (size_t)warp * kStages * ldr;
         uint64_t *bw = mbar + warp * kStages;
         const int nrows = warp < n ? (n - warp + NW - 1) / NW : 0;
-        auto row = [&](int t) { return warp + NW * (rev ? nrows - 1 - t : t); };
         const uint32_t bytes = (uint32_t)(ldh * sizeof(float));
         const int n4 = ldh >> 2;
         const float4 *X4 = (const float4 *)pxi, *C4 = (const float4 *)pc;
@@ -833,7 +829,7 @@ struct Opt {
         if (lane == 0) {
             for (int t = 0; t < nrows && t < kStages; ++t) {
                 mbar_expect_tx(&bw[t], bytes);
-                tma_load_row(rw + (size_t)t * ldr, H + (size_t)row(t) * ldh, bytes, &bw[t]);
+                tma_load_row(rw + (size_t)t * ldr, H + (size_t)(warp + NW * t) * ldh, bytes, &bw[t]);
             }
         }
         // groups of 4 row pairs: the 16 per-lane partial sums are reduced together
@@ -859,7 +855,7 @@ struct Opt {
                     aborted = true;
                     break;
                 }
-                const int i0 = row(t), i1 = two ? row(t + 1) : i0;
+                const int i0 = warp + NW * t, i1 = i0 + NW;
                 const float4 *A0 = (const float4 *)(rw + (size_t)s0 * ldr), *A1 = (const float4 *)(rw + (size_t)s1 * ldr);
                 float4 *W0 = (float4 *)(H + (size_t)i0 * ldh), *W1 = (float4 *)(H + (size_t)(two ? i1 : i0) * ldh);
                 const float r0 = pending ? (float)pr[i0] : 0.f, x0 = pending ? (float)pxi[i0] : 0.f;
@@ -895,11 +891,12 @@ struct Opt {
                     fence_proxy_async_smem();
                     if (t + kStages < nrows) {
                         mbar_expect_tx(&bw[s0], bytes);
-                        tma_load_row(rw + (size_t)s0 * ldr, H + (size_t)row(t + kStages) * ldh, bytes, &bw[s0]);
+                        tma_load_row(rw + (size_t)s0 * ldr, H + (size_t)(warp + NW * (t + kStages)) * ldh, bytes,
+                                     &bw[s0]);
                     }
                     if (t + 1 + kStages < nrows) {
                         mbar_expect_tx(&bw[s1], bytes);
-                        tma_load_row(rw + (size_t)s1 * ldr, H + (size_t)row(t + 1 + kStages) * ldh, bytes,
+                        tma_load_row(rw + (size_t)s1 * ldr, H + (size_t)(warp + NW * (t + 1 + kStages)) * ldh, bytes,
                                      &bw[s1]);
                     }
                 }
@@ -909,7 +906,7 @@ struct Opt {
             const float sum = reduce16(v);
             const int val = lane >> 1, tr = t0 + 2 * (val >> 2) + ((val >> 1) & 1);
             if (!(lane & 1) && tr < nrows) {
-                const int i = row(tr);
+                const int i = warp + NW * tr;
                 if (val & 1) hq[i] = sum;
                 else hp[i] = sum;
             }
@@ -1195,7 +1192,7 @@ struct Opt {
                 }
                 if (!LB) {
                     __syncthreads();
-                    if constexpr (!MSM && NC == 0 && sizeof(R) == 4) hpass_stream_v4(pending, (it & 1) != 0);
+                    if constexpr (!MSM && NC == 0 && sizeof(R) == 4) hpass_stream_v4(pending);
                     else if (MSM) hpass(pending);
                     else hpass_stream(pending);
                     __syncthreads();
@@ -1265,11 +1262,12 @@ struct Opt {
 
 // CTAs per SM a kernel instance is compiled for (its register budget): 2 for the
 // register-lean 256-thread dense BFGS instances (128 registers a thread, H columns
-// read from shared memory) and for the register-capped L-BFGS instance (NC = 0,
-// history in shared memory), 1 otherwise.  For L-BFGS, NC only selects the budget.
+// read from shared memory) and for the register-capped L-BFGS instances (NC = 0,
+// history in shared memory or in a global slot), 1 otherwise.  For L-BFGS, NC only
+// selects the budget.
 template <int NT, int NC, bool MSM, bool LB>
 constexpr int min_ctas() {
-    return (!LB && NC == 0 && NT <= 256) || (LB && MSM && NC == 0 && NT == 256) ? 2 : 1;
+    return (!LB && NC == 0 && NT <= 256) || (LB && NC == 0 && NT == 256) ? 2 : 1;
 }
 
 template <class R, class A, int NT, int NC, bool MSM, bool LB>

@@ -338,10 +338,12 @@ class Minimizer:
         return pos_dev.cpu().numpy(), e.cpu().numpy()
 
 
-# atom-count upper bounds of the size classes: each class maps to one kernel instance of the
-# default plan (256 threads / shared-memory H; 128 threads / shared-memory H; register-lean
-# global-slot H; L-BFGS or larger), so no two classes run the same instance
-DEFAULT_BINS = (24, 48, 170, 1024)
+# atom-count upper bounds of the size classes.  Dense BFGS (up to 170 atoms): each class runs
+# its own instance of the default plan (H in shared memory up to 24 and up to 48 atoms; the
+# register-lean global-slot H to 170).  L-BFGS: up to 170 atoms the register-capped instance
+# with the history in shared memory, 171-288 the register-capped one with the history in a
+# global slot (both two CTAs per SM), above that the uncapped one (one CTA per SM)
+DEFAULT_BINS = (24, 48, 170, 288, 1024)
 
 
 class BinnedMinimizer(Minimizer):
