@@ -15,6 +15,9 @@ class instead: ``--lo 4 --hi 8`` (up to 24 atoms), ``--lo 10 --hi 16``
 at most 20 rotatable bonds).  ``--lbfgs --mols 40 --k 8 --lo 60 --hi 75
 --max-atoms 170`` is one launch of the 150-170-atom class (320 conformers),
 whose instance keeps the L-BFGS history in shared memory at 2 CTAs per SM.
+``--lbfgs --keep-target --mols 40 --k 8 --lo 95 --hi 125 --max-atoms 288`` is one
+launch of the 171-288-atom class (186-284 atoms), whose instance keeps the history
+in a global slot at 2 CTAs per SM.
 
 Usage: python -m mlxmolkit_b200.profile_case [--mols 60] [--k 10] [--lo 8] [--hi 70] [--repeat 1]
                                              [--lbfgs] [--max-atoms 150]
@@ -41,11 +44,13 @@ def main():
     ap.add_argument("--hi", type=int, default=70, help="most heavy atoms")
     ap.add_argument("--lbfgs", action="store_true", help="L-BFGS m = 8 on large-workload-like molecules")
     ap.add_argument("--max-atoms", type=int, default=150)
+    ap.add_argument("--keep-target", action="store_true",
+                    help="with --lbfgs: the large workload's generator (heavy-atom count kept across redraws)")
     a = ap.parse_args()
     import torch
     if a.lbfgs:
         mols = synth.make_molecules(a.mols, a.k, a.seed, a.lo, a.hi, macro_frac=0.3, max_rotatable=20,
-                                    max_atoms=a.max_atoms, ring_density=0.12)
+                                    max_atoms=a.max_atoms, ring_density=0.12, keep_target=a.keep_target)
     else:
         mols = synth.make_molecules(a.mols, a.k, a.seed, a.lo, a.hi, max_atoms=a.max_atoms)
     hist, max_iters = (mm.LBFGS_M, 3000) if a.lbfgs else (0, 1000)
