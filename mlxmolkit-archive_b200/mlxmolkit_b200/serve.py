@@ -43,14 +43,16 @@ is bit-for-bit the same alone or in any mix of requests.
 | 49-149 with more than 32 non-bonded classes | dense BFGS | 149 | 64 |
 | 150-170 | L-BFGS m=8  | 170        | 32                |
 | 150-170 with more than 32 non-bonded classes | L-BFGS m=8 | 170 | 64 |
-| 171-300 | L-BFGS m=8  | 300        | 64                |
-| 301-400 | L-BFGS m=8  | 400        | 64                |
+| 171-288 | L-BFGS m=8  | 288        | 32                |
+| 171-288 with more than 32 non-bonded classes | L-BFGS m=8 | 288 | 64 |
+| 289-400 | L-BFGS m=8  | 400        | 64                |
 | > 400   | L-BFGS m=8  | its own    | 64                |
 
 Molecules of 150 atoms or more use L-BFGS, as in the reference pipeline
 (mlxmolkit/conformer_pipeline_v2.py:448-452), decided per molecule.  The
-150-170-atom L-BFGS class keeps its launch shape small (32 class-table
-entries) so that its instance fits two CTAs per SM, the register-capped one.
+150-170 and 171-288-atom L-BFGS classes keep their launch shape small (32
+class-table entries) so that their instances fit two CTAs per SM: the
+register-capped ones, with the history in shared memory and in a global slot.
 """
 from __future__ import annotations
 
@@ -103,8 +105,10 @@ def size_class(n_atoms: int, n_classes: int) -> SizeClass:
             if n_classes > 32:
                 return SizeClass(("lbfgs", 170, 64), 170, 64, mm.LBFGS_M)
             return SizeClass(("lbfgs", 170), 170, 32, mm.LBFGS_M)
-        if n_atoms <= 300:
-            return SizeClass(("lbfgs", 300), 300, 64, mm.LBFGS_M)
+        if n_atoms <= 288:
+            if n_classes > 32:
+                return SizeClass(("lbfgs", 288, 64), 288, 64, mm.LBFGS_M)
+            return SizeClass(("lbfgs", 288), 288, 32, mm.LBFGS_M)
         if n_atoms <= 400:
             return SizeClass(("lbfgs", 400), 400, 64, mm.LBFGS_M)
         return SizeClass(("lbfgs", n_atoms), n_atoms, 64, mm.LBFGS_M)

@@ -16,7 +16,7 @@ def _mols(n=6, k=3, seed=31, lo=8, hi=40, max_atoms=None):
 
 def _mixed_classes():
     """Molecules of every size class: <= 24, 25-48, 49-149 atoms (dense BFGS), 150-170 and
-    171-300 (L-BFGS)."""
+    171-288 (L-BFGS)."""
     small = _mols(n=3, k=3, seed=31, lo=4, hi=7)
     mid = _mols(n=3, k=3, seed=32, lo=10, hi=16)
     dense = _mols(n=3, k=2, seed=33, lo=30, hi=55, max_atoms=149)
@@ -31,7 +31,7 @@ def test_each_result_is_the_same_alone_and_in_the_mix_in_every_size_class():
     mols = _mixed_classes()
     n = [extract_mmff_params(m).n_atoms for m in mols]
     classes = {size_class(a, 10).key[:2] for a in n}
-    assert {("dense", 24), ("dense", 48), ("dense", 149), ("lbfgs", 170), ("lbfgs", 300)} <= classes, n
+    assert {("dense", 24), ("dense", 48), ("dense", 149), ("lbfgs", 170), ("lbfgs", 288)} <= classes, n
     alone = []
     srv = MMFFServer(hbm_budget_bytes=2 << 30)
     for m in mols:

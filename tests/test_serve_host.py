@@ -12,7 +12,9 @@ def test_size_classes_depend_only_on_the_molecule():
     assert serve.size_class(150, 10).history_m == 8                 # L-BFGS from 150 atoms
     assert serve.size_class(170, 10).key == ("lbfgs", 170) and serve.size_class(170, 10).max_classes == 32
     assert serve.size_class(160, 40).key == ("lbfgs", 170, 64)
-    assert serve.size_class(171, 10).nmax == 300
+    assert serve.size_class(171, 10).key == ("lbfgs", 288) and serve.size_class(288, 10).max_classes == 32
+    assert serve.size_class(200, 40).key == ("lbfgs", 288, 64)
+    assert serve.size_class(289, 10).nmax == 400
     assert serve.size_class(350, 10).nmax == 400
     assert serve.size_class(500, 10).nmax == 500
 
