@@ -161,6 +161,23 @@ int plan_minimize(const MMFFBatchDev *b, const MMFFConfDev *c, const MMFFOptPara
             pl->smem = L.total;
         }
     }
+    // mixed-precision L-BFGS where no two CTAs fit an SM (289 atoms and up): one CTA of 16 warps
+    // with the history in a global slot, where that layout fits (to about 410 atoms; decided
+    // with the full class table) -- 2 % faster on the large workload than 8 warps with the
+    // history in shared memory
+    if (mixed && lb && o->threads == 0 && pl->nc != 0) {
+        const Layout L16 = make_layout(nmax, 16, o->history_m, false, rs, as, 64);
+        if (L16.total <= (size_t)optin) {
+            pl->nt = 512;
+            pl->nc = 0;
+            pl->msm = false;
+            msm = false;
+            L = make_layout(nmax, 16, o->history_m, false, rs, as, mc);
+            pl->smem = L.total;
+            fit = occupancy();
+            if (fit < 0) return fit;
+        }
+    }
     if (o->ctas_per_sm > 0 && o->ctas_per_sm < fit) fit = o->ctas_per_sm;
     int grid = sms * fit;
     if (grid > c->n_conf) grid = c->n_conf > 0 ? c->n_conf : 1;

@@ -12,6 +12,7 @@ static int with_instance(const Plan &pl, bool lb, const Fn &fn) {
     using R = float;
     using A = double;
     if (lb) {
+        if (pl.nt == 512) return fn.template run<R, A, 512, 0, false, true>();   // 16 warps, global slot
         if (!pl.msm) return pl.nc == 0 ? fn.template run<R, A, 256, 0, false, true>()   // 128 registers
                                        : fn.template run<R, A, 256, 2, false, true>();
         return pl.nc == 0 ? fn.template run<R, A, 256, 0, true, true>()     // 128 registers, 2 CTAs/SM

@@ -61,9 +61,10 @@ def test_energy_and_gradient_match_the_oracle_at_large_sizes(golden_large, preci
 def test_first_iterations_follow_the_oracle(golden_large, hist, sel):
     """Step by step: after 25 iterations the FP64 kernel's energies equal the FP64 oracle's to
     rounding and the mixed kernel's to FP32 accuracy.  Dense: the streamed global-slot
-    instances.  Mixed L-BFGS, by the launch's atom bound: 377 atoms, the history in a global
-    slot (one CTA per SM); 178, the register-capped instance with the history in shared memory;
-    282, the register-capped instance with the history in a global slot (two CTAs per SM)."""
+    instances.  Mixed L-BFGS, by the launch's atom bound: 377 atoms, 512 threads with the
+    history in a global slot (one CTA of 16 warps per SM); 178, the register-capped instance
+    with the history in shared memory; 282, the register-capped instance with the history in a
+    global slot (two CTAs per SM)."""
     params, counts, pos = _batch(golden_large, sel)
     m = mm.Minimizer(params, counts)
     _, eo, _, io = oracle.minimize(params, counts, pos.astype(np.float64), max_iters=25, history_m=hist,
