@@ -114,14 +114,16 @@ def opt_params(max_iters: int, grad_tol: float, history_m: int = 0, precision: s
                atom_grad_scale: float = 1.0, max_restarts: int = 0,
                polish64: Optional[bool] = None, hpass_lean: bool = True, wait_spins: int = 0,
                err_word: int = 0, give_up_waits: bool = False) -> _lib.MMFFOptParams:
-    """Launch options; ``polish64`` switches a conformer's line-search energies to FP64 once the
-    FP32 ones stall.  Its default follows the optimizer: off for dense BFGS, whose mixed form is
-    then FP32 terms, gradients and update with FP64 only in the energy sums, the Armijo tests and
-    the convergence tests; on for mixed-precision L-BFGS, which on flexible 150-400-atom molecules
-    otherwise ends most conformers on an FP32 line-search stall short of the minimum.  ``err_word``: device address of an
-    int32 that the launch sets to 1 when a bounded wait gives up; ``wait_spins`` bounds those
-    waits (0: the library default); ``give_up_waits`` makes every such wait give up at once (a test
-    switch that exercises the timeout path)."""
+    """Launch options.
+
+    ``polish64`` switches a conformer's line-search energies to FP64 once the FP32 ones stall.
+    Its default follows the optimizer: off for dense BFGS, whose mixed form is then FP32 terms,
+    gradients and update with FP64 only in the energy sums, the Armijo tests and the
+    convergence tests; on for mixed-precision L-BFGS, which on flexible 150-400-atom molecules
+    otherwise ends most conformers on an FP32 line-search stall short of the minimum.
+    ``err_word``: device address of an int32 that the launch sets to 1 when a bounded wait gives
+    up; ``wait_spins`` bounds those waits (0: the library default); ``give_up_waits`` makes every
+    such wait give up at once (a test switch that exercises the timeout path)."""
     o = _lib.MMFFOptParams()
     o.wait_spins = int(wait_spins)
     o.give_up_waits = int(bool(give_up_waits))
@@ -540,13 +542,17 @@ def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, g
 
     Chunk r is packed (native, host threads), uploaded and launched on its own stream while
     the GPU runs chunks 0..r-1; streams get priorities in launch order, so a later chunk's
-    CTAs take SMs as an earlier chunk's work queue drains.  The call returns after its last
-    chunk's results are on the host.  Each chunk's FP64 check and
-    result copies follow its launch on the same stream.  Every chunk is planned at its size
-    class's atom bound, and the planner picks the kernel instance from the atom bound alone,
-    so a conformer's result is the same as in one ``BinnedMinimizer`` launch per class.  ``timings`` holds host seconds: ``setup_s`` until the first launch,
-    ``pack_s`` over all chunks (mostly overlapped), ``minimize_s`` from the first launch to the
-    last result, ``total_s``.
+    CTAs take SMs as an earlier chunk's work queue drains.  Each chunk's FP64 check and result
+    copies follow its launch on the same stream, and the call returns once every chunk's
+    results are on the host.
+
+    Every chunk is planned at its size class's atom bound, and the planner picks the kernel
+    instance from the atom bound alone, so a conformer's result is the same as in one
+    ``BinnedMinimizer`` launch per class.
+
+    ``timings`` holds host seconds: ``setup_s`` until the first launch, ``pack_s`` over all
+    chunks (mostly overlapped with the GPU), ``minimize_s`` from the first launch to the last
+    result, ``total_s``.
     """
     torch = _torch()
     t0 = time.perf_counter()
@@ -587,7 +593,7 @@ def minimize_pipelined(params_list, conf_counts, positions, *, max_iters: int, g
             if t_first is None:
                 t_first = time.perf_counter()
             e64, de, gr = m.fp64_check_device(x, e, stream=s)
-            host = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in (x, e, st, it, e64, de, gr, err)]
+            host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in (x, e, st, it, e64, de, gr, err)]
             for h, t in zip(host, (x, e, st, it, e64, de, gr, err)):
                 h.copy_(t, non_blocking=True)
             done = torch.cuda.Event()
